@@ -1,0 +1,124 @@
+// Internal device-side data structures and helpers of libggbtddft.
+//
+// Layout in HBM (per grid group g: runs that share N_r, N_l, the grid and W_l):
+//   x, y     [N_l][n_cols][N_r]  orbitals; column = one orbital of one run of the group.
+//            FP64 form: double2.  Split forms: float2.  For a single run this is the reference's
+//            d_x[l][kso*N_r + r] (main.cu:356-369) without the pointer-array indirection.
+//   W        radial propagators, FP64 form: double2 [N_l][N_r][N_r] = propagatorL%03d.bin.
+//   mats     angular chain matrices, [n_mats][N_m][N_l][ldS] doubles, stored so that the kernel's
+//            product is y[j] = sum_l S[l][j] x[l]  (S = A^T of the left multiplier A).
+//   dph      angular eigenvalues D[c][m][j], [4][N_m][ldS].
+//   coef     angular coefficient tables [COEF_N][N_m][N_l] (cu, cd, p, qu, qd, p3lm, f3lm).
+//   dens     density partials per column [n_cols][4][N_r] (not yet occupation weighted).
+//   obs      dipole/acceleration partials per column, l and r-tile [n_cols][N_l][n_tiles] double4.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ggb {
+
+constexpr int TR = 32;            // radii per angular tile (one warp-width, coalesced along r)
+constexpr int ANG_WARPS = 8;      // warps per angular CTA
+constexpr int MAX_NL = 256;       // largest N_l supported by the angular kernels
+constexpr int N_DEN = 4;          // density multipoles carried per column (L = 0..3)
+
+// status bits (sticky, OR-ed on the device)
+constexpr unsigned ST_NAN = 1u;
+constexpr unsigned ST_STEP_OVERFLOW = 2u;
+constexpr unsigned ST_NORM_GROWTH = 4u;
+
+enum PhaseKind { PH_NONE = 0, PH_P = 1, PH_FP = 2, PH_D = 3, PH_FF = 4 };
+enum Coef { CF_CU = 0, CF_CD = 1, CF_P = 2, CF_QU = 3, CF_QD = 4, CF_P3 = 5, CF_F3 = 6, COEF_N = 7 };
+
+struct ChainOp {
+  int mat;    // chain matrix index
+  int phase;  // PhaseKind applied to this product's outputs
+  int coupling;  // which eigenvalue set the phase uses (0..3)
+};
+
+// One half-step program: [S] (A_0, phase_0) (A_1, phase_1) ... (A_k) [S]
+struct Chain {
+  int n_ops;
+  int pre_s;
+  int post_s;
+  ChainOp ops[9];
+};
+
+struct RunDev {
+  const double* E;        // [n_t]
+  double* v;              // [4][N_r] Hartree multipoles (real part of the reference's d_v)
+  double* v0;             // [N_r]   t = 0 monopole
+  double* vexc;           // [N_r]
+  double* vexc0;          // [N_r]
+  const double* rho_frozen;  // [N_r]
+  double2* dip;           // per_l: [N_l][n_orb][n_t]
+  double2* acc;
+  double2* dip_tot;       // [n_orb][n_t]
+  double2* acc_tot;
+  double* norm;           // [n_orb][n_t]
+  double* norm0;          // [n_orb] norm at t = 0 (for the growth watchdog)
+  int col0;
+  int n_orb;
+  int n_t;
+  int flags;
+};
+
+struct GroupArgs {
+  int n_r, n_l, n_m, n_cols, n_tiles, ldS, n_runs;
+  int hartree_on;   // USE_HARTREE == 1 && targetID > 0
+  int p_hartree;    // P phase carries v_1 (USE_HARTREE && N_har > 1 && targetID > 0)
+  int n_den;        // multipoles computed: min(N_har, 4) when hartree_on, else 0
+  int per_l;
+  double dt;
+  double n_g_fac;   // N_g (N_g + 1) / 2
+  const double* r;
+  const double* drdx;
+  const double* P;
+  const double* mats;
+  const double* dph;
+  const double* coef;
+  const int* col_run;   // [n_cols] run index within ctx
+  const int* col_m;
+  const int* col_occ;
+  const int* runs_of_group;  // [n_runs] ctx run indices
+  RunDev* runs;             // ctx-wide device array
+  double* dens;
+  double4* obs;
+  int* step;                // ctx-wide step counter
+  unsigned* status;
+  unsigned* done;           // block counter for the last-block step increment
+  Chain chain[2];
+};
+
+__device__ __forceinline__ double2 cmul_conj_phase(double2 x, double eta) {
+  // x * exp(-i eta) written as the reference's phase kernels do (couplingP.cuh:99-102)
+  double s, c;
+  sincos(eta, &s, &c);
+  return make_double2(c * x.x + s * x.y, c * x.y - s * x.x);
+}
+
+// Double-double accumulation (Knuth TwoSum): used for the compensated Hartree prefix sums.
+struct dd {
+  double hi, lo;
+};
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+  double s = a.hi + b.hi;
+  double bp = s - a.hi;
+  double e = (a.hi - (s - bp)) + (b.hi - bp);
+  e += a.lo + b.lo;
+  double h = s + e;
+  return dd{h, e - (h - s)};
+}
+__device__ __forceinline__ dd dd_shfl_up(dd a, int d) {
+  return dd{__shfl_up_sync(0xffffffffu, a.hi, d), __shfl_up_sync(0xffffffffu, a.lo, d)};
+}
+
+// launchers (ggb_kernels_fp64.cu)
+void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
+                         cudaStream_t s);
+void launch_radial_fp64(const GroupArgs& g, const double2* W, const double2* xin, double2* xout,
+                        cudaStream_t s);
+void launch_finalize(const GroupArgs& g, int mode, cudaStream_t s);
+size_t angular_smem_fp64(int n_l);
+
+}  // namespace ggb

@@ -1,0 +1,543 @@
+// FP64 (parity form) kernels of the split-operator step.
+//
+//  k_angular_fp64  one half of the angular step for a tile of 32 radii of one orbital column:
+//                  the whole l-vector of every radius is held in shared memory while the chain
+//                  (rotate -> phase -> [pre-multiplied rotate pair] -> phase ... -> rotate back,
+//                  plus the l-diagonal S phase) is applied.  Replaces, per half-step, the 3
+//                  launches of each of h_couplingFF/FP/D/P (couplingP.cuh:108-125, couplingD.cuh,
+//                  couplingF.cuh) and h_couplingS (couplingS.cuh:43-57).  The second half also
+//                  produces the density-multipole and dipole/acceleration partial sums of the new
+//                  orbitals (hartreePotentialDensity.cuh:1-181, dipoleMoment.cuh:1-75,
+//                  dipoleAcceleration.cuh:1-71), so the orbitals are read once per half-step.
+//  k_radial_fp64   x_l <- A_l x_l for every l with A_l(a,b) = W[l][b][a]: the batched ZGEMM of
+//                  h_propagationH0 (h_timePropagation.cuh:1-30), out of place.
+//  k_finalize      per run: observables of the step from the partials, density multipoles
+//                  (occupation-weighted sum over orbitals), Hartree potentials by compensated
+//                  prefix scans (h_calculateHartreePotential.cuh:1-136), LDA exchange
+//                  (h_calculateExchangeCorrelationPotential.cuh:1-56), step counter.
+#include <cstdio>
+#include "ggb_internal.cuh"
+
+namespace ggb {
+
+// ---------------------------------------------------------------------------------------------
+// angular chain
+// ---------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ double cf(const double* tab, int n_l, int l) {
+  return (l >= 0 && l < n_l) ? tab[l] : 0.0;
+}
+
+__device__ __forceinline__ double xdot(const double2* xs, int n_l, int a, int b, int lane) {
+  if (a < 0 || a >= n_l || b < 0 || b >= n_l) return 0.0;
+  const double2 xa = xs[a * TR + lane];
+  const double2 xb = xs[b * TR + lane];
+  return xa.x * xb.x + xa.y * xb.y;
+}
+
+// One multipole of one orbital's density at one radius, with the reference's literal l ranges
+// (hartreePotentialDensity.cuh:21-177, including the tail loop of L = 3 that restarts at N_l-4).
+__device__ double density_multipole(int L, int m, int n_l, const double2* xs, int lane,
+                                    const double* coef, int n_m) {
+  const double* cu = coef + ((size_t)CF_CU * n_m + m) * n_l;
+  const double* cd = coef + ((size_t)CF_CD * n_m + m) * n_l;
+  const double* pp = coef + ((size_t)CF_P * n_m + m) * n_l;
+  const double* qu = coef + ((size_t)CF_QU * n_m + m) * n_l;
+  const double* qd = coef + ((size_t)CF_QD * n_m + m) * n_l;
+  const double* p3 = coef + ((size_t)CF_P3 * n_m + m) * n_l;
+  const double* f3 = coef + ((size_t)CF_F3 * n_m + m) * n_l;
+  double d = 0.0;
+  if (L == 0) {
+    for (int lp = m; lp < n_l; ++lp) {
+      const double2 v = xs[lp * TR + lane];
+      d += v.x * v.x + v.y * v.y;
+    }
+  } else if (L == 1) {
+    int lp = m;
+    d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
+    for (lp = m + 1; lp < n_l - 1; ++lp)
+      d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+    lp = n_l - 1;
+    d += cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+  } else if (L == 2) {
+    for (int lp = m; lp < m + 2; ++lp)
+      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+    for (int lp = m + 2; lp < n_l - 2; ++lp)
+      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) +
+           cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+    for (int lp = n_l - 2; lp < n_l; ++lp)
+      d += cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+  } else if (L == 3) {
+    int lp = m;
+    d += cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = m + 1; lp < m + 3; ++lp)
+      d += cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) + cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) +
+           cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = m + 3; lp < n_l - 3; ++lp)
+      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = n_l - 4; lp < n_l - 1; ++lp)
+      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
+    d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane);
+  }
+  return d;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Dipole and acceleration partial sums over this tile's radii for every l of one column
+// (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc).
+__device__ void observables_tile(const GroupArgs& g, const double2* xs, int col, int m, int tile, int lane,
+                                 int warp, double rr, double fr2) {
+  const int n_l = g.n_l;
+  const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
+  const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
+  for (int l = warp; l < n_l; l += ANG_WARPS) {
+    double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (l >= m) {
+      const double2 xl = xs[l * TR + lane];
+      const double2 xu = (l + 1 < n_l) ? xs[(l + 1) * TR + lane] : make_double2(0.0, 0.0);
+      const double2 xd = (l >= 1) ? xs[(l - 1) * TR + lane] : make_double2(0.0, 0.0);
+      const double c_u = cu[l], c_d = cd[l];
+      double2 z1, z2;
+      if (l == m) {
+        z1 = make_double2(rr * c_u * xu.x, rr * c_u * xu.y);
+        z2 = make_double2(fr2 * c_u * xu.x, fr2 * c_u * xu.y);
+      } else if (l == n_l - 1) {
+        z1 = make_double2(rr * c_d * xd.x, rr * c_d * xd.y);
+        z2 = make_double2(fr2 * c_d * xd.x, fr2 * c_d * xd.y);
+      } else {
+        z1 = make_double2(rr * c_u * xu.x + rr * c_d * xd.x, rr * c_u * xu.y + rr * c_d * xd.y);
+        z2 = make_double2(fr2 * (c_u * xu.x + c_d * xd.x), fr2 * (c_u * xu.y + c_d * xd.y));
+      }
+      // conj(x_l) . z
+      out.x = xl.x * z1.x + xl.y * z1.y;
+      out.y = xl.x * z1.y - xl.y * z1.x;
+      out.z = xl.x * z2.x + xl.y * z2.y;
+      out.w = xl.x * z2.y - xl.y * z2.x;
+    }
+    out.x = warp_sum(out.x);
+    out.y = warp_sum(out.y);
+    out.z = warp_sum(out.z);
+    out.w = warp_sum(out.w);
+    if (lane == 0) g.obs[((size_t)col * n_l + l) * g.n_tiles + tile] = out;
+  }
+}
+
+constexpr int ANG_JB = 8;   // eigen-channels j per register block
+
+__global__ void __launch_bounds__(ANG_WARPS * 32)
+k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* __restrict__ xout, int do_obs) {
+  extern __shared__ double2 sm[];  // two [N_l][TR] buffers
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int col = blockIdx.x / g.n_tiles;
+  const int tile = blockIdx.x - col * g.n_tiles;
+  const int r = tile * TR + lane;
+  const bool rv = r < g.n_r;
+  const int n_l = g.n_l;
+  double2* xs = sm;
+  double2* ys = sm + (size_t)n_l * TR;
+  const int m = g.col_m[col];
+  const RunDev run = g.runs[g.col_run[col]];
+  int step = *g.step;
+  if (step >= run.n_t) step = run.n_t - 1;  // overflow is flagged by k_finalize
+
+  for (int l = warp; l < n_l; l += ANG_WARPS)
+    xs[l * TR + lane] = rv ? xin[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
+
+  // per-radius potentials
+  const double rr = rv ? g.r[r] : 1.0;
+  const int rc = rv ? r : 0;
+  const double E = run.E[step];
+  double v1 = 0.0, v2 = 0.0, v3 = 0.0, sbase = 0.0;
+  if (g.hartree_on) {
+    v1 = run.v[1 * g.n_r + rc];
+    v2 = run.v[2 * g.n_r + rc];
+    v3 = run.v[3 * g.n_r + rc];
+    // couplingS.cuh:20-21, evaluated left to right
+    sbase = run.v[rc] - run.v0[rc] + run.vexc[rc] - run.vexc0[rc];
+  }
+  const double hdt = 0.5 * g.dt;
+  const double* pco = g.coef + ((size_t)CF_P * g.n_m + m) * n_l;
+  __syncthreads();
+
+  const Chain& ch = g.chain[half];
+  if (ch.pre_s) {
+    for (int l = warp; l < n_l; l += ANG_WARPS) {
+      double eta = sbase + pco[l] * v2;
+      eta *= hdt;
+      xs[l * TR + lane] = cmul_conj_phase(xs[l * TR + lane], eta);
+    }
+    __syncthreads();
+  }
+
+  for (int o = 0; o < ch.n_ops; ++o) {
+    const ChainOp op = ch.ops[o];
+    const double* S = g.mats + ((size_t)op.mat * g.n_m + m) * (size_t)n_l * g.ldS;
+    const bool last = (o == ch.n_ops - 1);
+    double base = 0.0;
+    if (op.phase == PH_P) base = g.p_hartree ? (rr * E + v1) : (rr * E);
+    else if (op.phase == PH_D) base = v2;
+    else if (op.phase != PH_NONE) base = v3;  // FP and FF
+    const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
+    for (int j0 = warp * ANG_JB; j0 < n_l; j0 += ANG_WARPS * ANG_JB) {
+      double2 acc[ANG_JB];
+#pragma unroll
+      for (int q = 0; q < ANG_JB; ++q) acc[q] = make_double2(0.0, 0.0);
+      const double* Sc = S + j0;
+      for (int l = m; l < n_l; ++l) {
+        const double2 xv = xs[l * TR + lane];
+        const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)l * g.ldS);
+#pragma unroll
+        for (int h = 0; h < ANG_JB / 2; ++h) {
+          const double2 sv = __ldg(Srow + h);
+          acc[2 * h].x += sv.x * xv.x;     acc[2 * h].y += sv.x * xv.y;
+          acc[2 * h + 1].x += sv.y * xv.x; acc[2 * h + 1].y += sv.y * xv.y;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < ANG_JB; ++q) {
+        const int j = j0 + q;
+        if (j < n_l) {
+          double2 y = acc[q];
+          // phase in the eigenbasis (couplingP.cuh:61-106 and twins)
+          if (op.phase != PH_NONE && j >= m) {
+            double eta = base;
+            eta *= hdt * Dv[j];
+            y = cmul_conj_phase(y, eta);
+          }
+          if (last && ch.post_s) {
+            double eta = sbase + pco[j] * v2;
+            eta *= hdt;
+            y = cmul_conj_phase(y, eta);
+          }
+          ys[j * TR + lane] = y;
+        }
+      }
+    }
+    __syncthreads();
+    double2* t = xs; xs = ys; ys = t;
+  }
+
+  if (rv)
+    for (int l = warp; l < n_l; l += ANG_WARPS) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * TR + lane];
+
+  if (do_obs) {
+    const double fr2 = rv ? pow(rr, -2.0) : 0.0;
+    observables_tile(g, xs, col, m, tile, lane, warp, rr, fr2);
+    const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
+    for (int L = warp; L < n_den; L += ANG_WARPS) {
+      const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
+      if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
+    }
+  }
+}
+
+size_t angular_smem_fp64(int n_l) { return 2 * (size_t)n_l * TR * sizeof(double2); }
+
+void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
+                         cudaStream_t s) {
+  const dim3 grid(g.n_cols * g.n_tiles), block(ANG_WARPS * 32);
+  const size_t smem = angular_smem_fp64(g.n_l);
+  cudaFuncSetAttribute(k_angular_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_angular_fp64<<<grid, block, smem, s>>>(g, half, xin, xout, do_obs);
+}
+
+// ---------------------------------------------------------------------------------------------
+// radial propagator, FP64
+// ---------------------------------------------------------------------------------------------
+
+constexpr int RAD_TI = 128;   // rows per CTA
+constexpr int RAD_KC = 32;    // k chunk staged in shared memory
+
+template <int TC>
+__global__ void __launch_bounds__(RAD_TI)
+k_radial_fp64(int n_r, int n_cols, const double2* __restrict__ W, const double2* __restrict__ xin,
+              double2* __restrict__ xout) {
+  __shared__ double2 xsm[TC][RAD_KC];
+  const int l = blockIdx.z;
+  const int i = blockIdx.x * RAD_TI + threadIdx.x;
+  const int c0 = blockIdx.y * TC;
+  const bool iv = i < n_r;
+  const double2* Wl = W + (size_t)l * n_r * n_r;
+  const double2* Xl = xin + (size_t)l * n_cols * n_r;
+  double2 acc[TC];
+#pragma unroll
+  for (int c = 0; c < TC; ++c) acc[c] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < n_r; k0 += RAD_KC) {
+    for (int idx = threadIdx.x; idx < TC * RAD_KC; idx += RAD_TI) {
+      const int c = idx / RAD_KC, kk = idx - c * RAD_KC;
+      xsm[c][kk] = (c0 + c < n_cols && k0 + kk < n_r) ? Xl[(size_t)(c0 + c) * n_r + k0 + kk] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int kmax = min(RAD_KC, n_r - k0);
+    for (int kk = 0; kk < kmax; ++kk) {
+      const double2 w = iv ? __ldcs(Wl + (size_t)(k0 + kk) * n_r + i) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        const double2 x = xsm[c][kk];
+        acc[c].x += w.x * x.x - w.y * x.y;
+        acc[c].y += w.x * x.y + w.y * x.x;
+      }
+    }
+    __syncthreads();
+  }
+  if (iv)
+#pragma unroll
+    for (int c = 0; c < TC; ++c)
+      if (c0 + c < n_cols) xout[((size_t)l * n_cols + c0 + c) * n_r + i] = acc[c];
+}
+
+void launch_radial_fp64(const GroupArgs& g, const double2* W, const double2* xin, double2* xout, cudaStream_t s) {
+  const int nc = g.n_cols;
+  int tc = nc >= 16 ? 16 : nc;
+  static const int opts[] = {1, 2, 3, 4, 6, 8, 9, 12, 16};
+  for (int o : opts)
+    if (o >= tc) { tc = o; break; }
+  const dim3 grid((g.n_r + RAD_TI - 1) / RAD_TI, (nc + tc - 1) / tc, g.n_l), block(RAD_TI);
+#define GGB_RAD_CASE(C) \
+  case C: k_radial_fp64<C><<<grid, block, 0, s>>>(g.n_r, nc, W, xin, xout); break;
+  switch (tc) {
+    GGB_RAD_CASE(1) GGB_RAD_CASE(2) GGB_RAD_CASE(3) GGB_RAD_CASE(4) GGB_RAD_CASE(6)
+    GGB_RAD_CASE(8) GGB_RAD_CASE(9) GGB_RAD_CASE(12) GGB_RAD_CASE(16)
+    default: break;
+  }
+#undef GGB_RAD_CASE
+}
+
+// ---------------------------------------------------------------------------------------------
+// finalize: observables, Hartree multipoles (compensated scans), exchange, step counter
+// ---------------------------------------------------------------------------------------------
+
+constexpr int FIN_THREADS = 256;
+
+// Inclusive (forward) or suffix-exclusive (backward) compensated scan of t[0..n) in shared memory.
+// forward:  out[a] = sum_{b <= a} t[b]      backward: out[a] = sum_{b > a} t[b]
+__device__ void block_scan_dd(const double* t, double* out, int n, bool backward, dd* wsum) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = FIN_THREADS / 32;
+  const int per = (n + FIN_THREADS - 1) / FIN_THREADS;
+  const int b0 = tid * per;
+  // local inclusive sums in the scan direction
+  dd loc{0.0, 0.0};
+  for (int q = 0; q < per; ++q) {
+    const int k = b0 + q;
+    if (k < n) loc = dd_add(loc, dd{t[backward ? n - 1 - k : k], 0.0});
+  }
+  // warp inclusive scan of thread totals
+  dd inc = loc;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    dd o = dd_shfl_up(inc, d);
+    if (lane >= d) inc = dd_add(o, inc);
+  }
+  if (lane == 31) wsum[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    dd w = lane < nw ? wsum[lane] : dd{0.0, 0.0};
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      dd o = dd_shfl_up(w, d);
+      if (lane >= d) w = dd_add(o, w);
+    }
+    if (lane < nw) wsum[lane] = w;
+  }
+  __syncthreads();
+  // exclusive prefix of this thread = inclusive value of the previous lane + earlier warps
+  const dd prev = dd_shfl_up(inc, 1);
+  dd run = lane == 0 ? dd{0.0, 0.0} : prev;
+  if (warp > 0) run = dd_add(wsum[warp - 1], run);
+  for (int q = 0; q < per; ++q) {
+    const int k = b0 + q;
+    if (k < n) {
+      const int idx = backward ? n - 1 - k : k;
+      const double tv = t[idx];
+      if (backward) {
+        out[idx] = run.hi + run.lo;                 // exclusive (sum over b > a)
+        run = dd_add(run, dd{tv, 0.0});
+      } else {
+        run = dd_add(run, dd{tv, 0.0});
+        out[idx] = run.hi + run.lo;                 // inclusive (sum over b <= a)
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double ipow(double x, int L) {
+  double p = 1.0;
+  for (int i = 0; i < L; ++i) p *= x;
+  return p;
+}
+
+// Blocks: for each run of the group, n_den Hartree blocks (L = 0..n_den-1; block L = 0 also does
+// the exchange potential) + 1 observables block.  mode 0 = initial potentials (no observables,
+// no step increment), mode 1 = end of step.
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode) {
+  extern __shared__ double fsm[];  // [3][N_r]
+  __shared__ dd wsum[FIN_THREADS / 32];
+  const int nb = g.n_den + 1;
+  const int ri = blockIdx.x / nb;
+  const int role = blockIdx.x - ri * nb;  // < n_den: Hartree L = role; == n_den: observables
+  const int run_idx = g.runs_of_group[ri];
+  RunDev run = g.runs[run_idx];
+  const int n_r = g.n_r, n_l = g.n_l, tid = threadIdx.x;
+  const int step = *g.step;
+  const bool obs_block = (role == g.n_den);
+
+  if (obs_block && mode == 1) {
+    if (step >= run.n_t) {
+      if (tid == 0) atomicOr(g.status, ST_STEP_OVERFLOW);
+    } else {
+      const int n_orb = run.n_orb;
+      // per (l, orbital): sum over r tiles
+      for (int idx = tid; idx < n_l * n_orb; idx += FIN_THREADS) {
+        const int l = idx / n_orb, k = idx - l * n_orb;
+        const double4* p = g.obs + ((size_t)(run.col0 + k) * n_l + l) * g.n_tiles;
+        double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int t = 0; t < g.n_tiles; ++t) {
+          const double4 v = p[t];
+          s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        }
+        if (g.per_l) {
+          run.dip[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(s.x, s.y);
+          run.acc[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(s.z, s.w);
+        }
+      }
+      // per orbital: totals over l and the norm; one warp per orbital
+      const int lane = tid & 31, warp = tid >> 5;
+      for (int k = warp; k < n_orb; k += FIN_THREADS / 32) {
+        const double4* p = g.obs + (size_t)(run.col0 + k) * n_l * g.n_tiles;
+        double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int q = lane; q < n_l * g.n_tiles; q += 32) {
+          const double4 v = p[q];
+          s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+        }
+        s.x = warp_sum(s.x); s.y = warp_sum(s.y); s.z = warp_sum(s.z); s.w = warp_sum(s.w);
+        const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;  // L = 0 row
+        double nrm = 0.0;
+        for (int q = lane; q < n_r; q += 32) nrm += dn[q];
+        nrm = warp_sum(nrm);
+        if (lane == 0) {
+          run.dip_tot[(size_t)k * run.n_t + step] = make_double2(s.x, s.y);
+          run.acc_tot[(size_t)k * run.n_t + step] = make_double2(s.z, s.w);
+          run.norm[(size_t)k * run.n_t + step] = nrm;
+          if (!(nrm == nrm) || isinf(nrm) || !(s.x == s.x) || !(s.z == s.z)) atomicOr(g.status, ST_NAN);
+          if (nrm > run.norm0[k] * (1.0 + 1e-6) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
+        }
+      }
+    }
+  } else if (obs_block && mode == 0) {
+    // initial norm for the growth watchdog
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int k = warp; k < run.n_orb; k += FIN_THREADS / 32) {
+      const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;
+      double nrm = 0.0;
+      for (int q = lane; q < n_r; q += 32) nrm += dn[q];
+      nrm = warp_sum(nrm);
+      if (lane == 0) run.norm0[k] = nrm;
+    }
+  }
+
+  if (!obs_block) {
+    const int L = role;
+    double* rho = fsm;            // [N_r]
+    double* F = fsm + n_r;        // forward partial sums
+    double* G = fsm + 2 * n_r;    // backward partial sums
+    // rho_L(r) = sum_kso occ * density_kso (hartreePotentialDensity.cuh:58-60, orbital order)
+    for (int q = tid; q < n_r; q += FIN_THREADS) {
+      double s = 0.0;
+      for (int k = 0; k < run.n_orb; ++k)
+        s += (double)g.col_occ[run.col0 + k] * g.dens[((size_t)(run.col0 + k) * N_DEN + L) * n_r + q];
+      rho[q] = s;
+    }
+    __syncthreads();
+    // v_L(r_a) = r_a^-(L+1) sum_{b<=a} rho(b) r_b^L + r_a^L sum_{b>a} rho(b) r_b^-(L+1)
+    for (int q = tid; q < n_r; q += FIN_THREADS) {
+      const double rb = g.r[q];
+      F[q] = rho[q] * ipow(rb, L);
+      G[q] = rho[q] / ipow(rb, L + 1);
+    }
+    __syncthreads();
+    block_scan_dd(F, F, n_r, false, wsum);
+    block_scan_dd(G, G, n_r, true, wsum);
+    for (int q = tid; q < n_r; q += FIN_THREADS) {
+      const double ra = g.r[q];
+      const double v = F[q] / ipow(ra, L + 1) + ipow(ra, L) * G[q];
+      run.v[(size_t)L * n_r + q] = v;
+      if (mode == 0 && L == 0) run.v0[q] = v;
+    }
+  }
+
+  // exchange (block L = 0, or the observables block when Hartree is off)
+  const bool xc_block = (g.n_den > 0) ? (role == 0) : obs_block;
+  if (xc_block) {
+    const bool pw92 = (run.flags & 1) != 0;
+    for (int q = tid; q < n_r; q += FIN_THREADS) {
+      double rho0 = 0.0;
+      if (g.n_den > 0) rho0 = fsm[q];
+      // h_calculateExchangeCorrelationPotential.cuh:33-44
+      double den = g.n_g_fac * (rho0 / 4.0 / M_PI + run.rho_frozen[q]) / g.drdx[q] * pow(g.P[q], 2.0);
+      const double rq = g.r[q];
+      if (mode == 0) {
+        double vx0 = -pow(3.0 / M_PI * den, 1.0 / 3.0);
+        vx0 /= pow(rq, 2.0 / 3.0);
+        if (pw92) {
+          // PW92 correlation of n = den / r^2 (not in the reference)
+          const double n = fmax(den / (rq * rq), 1e-300);
+          const double a = 0.031091, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+          const double rs = cbrt(3.0 / (4.0 * M_PI * n)), srs = sqrt(rs);
+          const double q0 = -2.0 * a * (1.0 + a1 * rs);
+          const double q1 = 2.0 * a * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs);
+          const double q1p = a * (b1 / srs + 2.0 * b2 + 3.0 * b3 * srs + 4.0 * b4 * rs);
+          const double lg = log1p(1.0 / q1);
+          vx0 += q0 * lg - rs / 3.0 * (-2.0 * a * a1 * lg - q0 * q1p / (q1 * q1 + q1));
+        }
+        run.vexc0[q] = vx0;
+      }
+      if (den < 0.0) den = 0.0;
+      double vx = -pow(3.0 / M_PI * den, 1.0 / 3.0);
+      vx /= pow(rq, 2.0 / 3.0);
+      if (pw92) {
+        const double n = fmax(den / (rq * rq), 1e-300);
+        const double a = 0.031091, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+        const double rs = cbrt(3.0 / (4.0 * M_PI * n)), srs = sqrt(rs);
+        const double q0 = -2.0 * a * (1.0 + a1 * rs);
+        const double q1 = 2.0 * a * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs);
+        const double q1p = a * (b1 / srs + 2.0 * b2 + 3.0 * b3 * srs + 4.0 * b4 * rs);
+        const double lg = log1p(1.0 / q1);
+        vx += q0 * lg - rs / 3.0 * (-2.0 * a * a1 * lg - q0 * q1p / (q1 * q1 + q1));
+      }
+      run.vexc[q] = vx;
+    }
+  }
+
+  // last block of a step advances the shared step counter
+  if (mode == 1) {
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      const unsigned total = gridDim.x;
+      const unsigned prev = atomicAdd(g.done, 1u);
+      if (prev == total - 1) {
+        *g.done = 0u;
+        __threadfence();
+        atomicAdd(g.step, 1);
+      }
+    }
+  }
+}
+
+void launch_finalize(const GroupArgs& g, int mode, cudaStream_t s) {
+  const dim3 grid(g.n_runs * (g.n_den + 1)), block(FIN_THREADS);
+  const size_t smem = 3 * (size_t)g.n_r * sizeof(double);
+  cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_finalize<<<grid, block, smem, s>>>(g, mode);
+}
+
+}  // namespace ggb

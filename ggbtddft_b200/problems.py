@@ -1,0 +1,244 @@
+"""Run definitions: everything one atom-in-field run needs, built from the input producers.
+
+A ``RunInputs`` holds the same arrays the reference's ``main.cu`` loads from ``workingData``
+plus its compile-time scalars (``src/params.cuh:25-60``):
+
+    grid (r, drdx, P)                    workingData/mesh/{r,drdx,P}.bin
+    W [N_l][N_r][N_r] complex128         workingData/hamiltonian/propagators/propagatorL%03d.bin
+    V/D per coupling [N_m][N_l][N_l]     workingData/hamiltonian/propagatorsL/<c>/V%03d.bin, D%03d.bin
+    x0 [N_l][n_orb][N_r] complex128      workingData/eigenStates/active/<id>/eigenStatesL%03d.bin
+    l/m/occ [n_orb] int32, rho_frozen    workingData/stateParameters/*.bin
+    E [N_t]                              h_initialiseField (host-computed)
+
+Named builders produce the benchmark configurations with seeded synthetic laser parameters.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import inputs as I
+
+
+@dataclasses.dataclass
+class RunInputs:
+    grid: I.RadialGrid
+    n_l: int
+    dt: float
+    W: np.ndarray
+    V: Dict[str, np.ndarray]
+    D: Dict[str, np.ndarray]
+    x0: np.ndarray
+    l_active: np.ndarray
+    m_active: np.ndarray
+    occ: np.ndarray
+    rho_frozen: np.ndarray
+    E: np.ndarray
+    n_har: int = 4
+    use_hartree: int = 1
+    target_id: int = 0
+    xc_correlation: bool = False
+    name: str = ""
+    omega0: float = 0.057
+
+    @property
+    def n_r(self) -> int:
+        return self.grid.n_r
+
+    @property
+    def n_orb(self) -> int:
+        return self.x0.shape[1]
+
+    @property
+    def n_t(self) -> int:
+        return self.E.size
+
+    @property
+    def n_m(self) -> int:
+        return int(self.m_active.max()) + 1
+
+    def with_field(self, E: np.ndarray) -> "RunInputs":
+        return dataclasses.replace(self, E=np.ascontiguousarray(E, dtype=np.float64))
+
+
+def initial_orbitals(gs: I.GroundState, n_l: int) -> np.ndarray:
+    """x[l][kso][r]: orbital kso placed in its own l, zero elsewhere (h_initialiseTDKSOSet.cuh:59-84)."""
+    n_orb = len(gs.orbitals)
+    x = np.zeros((n_l, n_orb, gs.u.shape[1]), dtype=np.complex128)
+    for k, o in enumerate(gs.orbitals):
+        x[o.l, k, :] = gs.u[k]
+    return x
+
+
+def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.ndarray, *,
+              absorber: str = "cap", cap_r_mask: Optional[float] = None, cap_passes: int = 2,
+              mask_width: Optional[float] = None, n_har: int = 4, use_hartree: int = 1,
+              target_id: int = 0, xc_correlation: bool = False, name: str = "",
+              omega0: float = 0.057, device: Optional[str] = None,
+              W: Optional[np.ndarray] = None) -> RunInputs:
+    """Assemble one run.
+
+    absorber = "cap":  the reference's Manolopoulos CAP starting at ``cap_r_mask``, entering the
+                       Hamiltonian ``cap_passes`` times (2 reproduces v0 - i W - i maskR,
+                       groundState.py:27 + internal.py:253).
+    absorber = "mask": a cos^(1/8) mask over the last ``mask_width`` a.u. folded into W's rows.
+    """
+    r = grid.r
+    if absorber == "cap":
+        r_mask = cap_r_mask if cap_r_mask is not None else grid.r_max / 1.5
+        cap = I.cap_manolopoulos(r, r_mask, grid.r_max)
+        v0 = gs.v_ion - 1j * cap * (cap_passes - 1)
+        mask_r = cap
+        row_mask = None
+    elif absorber == "mask":
+        v0 = gs.v_ion.astype(np.complex128)
+        mask_r = np.zeros_like(r)
+        row_mask = I.mask_cos8(r, grid.r_max, mask_width)
+    elif absorber == "none":
+        v0 = gs.v_ion.astype(np.complex128)
+        mask_r = np.zeros_like(r)
+        row_mask = None
+    else:
+        raise ValueError(absorber)
+    if W is None:
+        W = I.radial_propagators(grid, n_l, dt, v0, gs.vscf, mask_r, row_mask=row_mask, device=device)
+    n_m = int(max(o.m for o in gs.orbitals)) + 1
+    ang = I.angular_eigensystems(n_l, n_m)
+    return RunInputs(
+        grid=grid, n_l=n_l, dt=dt, W=W,
+        V={c: ang[c][0] for c in I.COUPLINGS}, D={c: ang[c][1] for c in I.COUPLINGS},
+        x0=initial_orbitals(gs, n_l),
+        l_active=np.array([o.l for o in gs.orbitals], dtype=np.int32),
+        m_active=np.array([o.m for o in gs.orbitals], dtype=np.int32),
+        occ=np.array([o.occ for o in gs.orbitals], dtype=np.int32),
+        rho_frozen=gs.rho_frozen.copy(), E=np.ascontiguousarray(E, dtype=np.float64),
+        n_har=n_har, use_hartree=use_hartree, target_id=target_id,
+        xc_correlation=xc_correlation, name=name, omega0=omega0)
+
+
+# ----------------------------------------------------------------------------------------------
+# small, reference-shaped problems (multiples of 32 so that the reference binary covers them too)
+# ----------------------------------------------------------------------------------------------
+
+def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H", *,
+                   r_mask: float = 30.0, zeta_ref: float = 1.0, dt_as: float = 20.0,
+                   intensity: float = 2e14, omega0: float = 0.057, cycles: float = 1.0,
+                   cep: float = 0.5 * math.pi, n_har: int = 4, use_hartree: int = 1,
+                   seed: int = 0, perturb: float = 0.0) -> RunInputs:
+    """A run built the way the reference's init.py builds one (CAP twice, super-Gaussian, CN).
+
+    atom "H": hydrogen-like 1s, targetID 0 (no Hartree/XC in the loop).
+    atom "Ne3": a 3-orbital LDA atom (1s, 2p0, 2p1; occ 2,2,4; targetID 2) so that every
+    coupling (P, FP, D, FF, S), the Hartree multipoles and the exchange potential are active.
+    ``perturb`` mixes seeded random noise into the initial orbitals (then renormalises) so that
+    the parity tests also exercise components that vanish for exact eigenstates.
+    """
+    r_max = 1.5 * r_mask
+    grid = I.make_grid(n_r, r_max, zeta_ref)
+    dt = dt_as * I.ATTOSECOND_AU
+    if atom == "H":
+        gs = I.ground_state(grid, 1.0, I.ORBITALS_H, interacting=False)
+        target_id = 0
+    elif atom == "Ne3":
+        orbs = [I.Orbital(1, 0, 0, 2), I.Orbital(2, 1, 0, 2), I.Orbital(2, 1, 1, 4)]
+        gs = I.ground_state(grid, 8.0, orbs, interacting=True, iterations=60)
+        target_id = 2
+    else:
+        raise ValueError(atom)
+    if perturb:
+        rng = np.random.default_rng(seed)
+        u = gs.u + perturb * rng.standard_normal(gs.u.shape) * np.abs(gs.u).max(axis=1, keepdims=True)
+        u /= np.sqrt((u ** 2).sum(axis=1, keepdims=True))
+        gs = dataclasses.replace(gs, u=u)
+    t = I.time_grid(n_t, dt)
+    e0 = I.intensity_to_e0(intensity)
+    tau0 = cycles * 2.0 * math.pi / omega0
+    E = I.field_super_gaussian(t, e0, omega0, tau0, cep)
+    return build_run(grid, n_l, dt, gs, E, absorber="cap", cap_r_mask=r_mask, cap_passes=2,
+                     n_har=n_har, use_hartree=use_hartree, target_id=target_id,
+                     name=f"{atom}-N{n_r}-L{n_l}", omega0=omega0)
+
+
+# ----------------------------------------------------------------------------------------------
+# benchmark configurations
+# ----------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class LaserSpec:
+    intensity: float      # W/cm^2
+    wavelength_nm: float
+    cycles: float
+    cep: float = 0.0
+
+    @property
+    def omega(self) -> float:
+        return I.wavelength_to_omega(self.wavelength_nm)
+
+    @property
+    def e0(self) -> float:
+        return I.intensity_to_e0(self.intensity)
+
+
+@dataclasses.dataclass
+class AtomSpec:
+    name: str
+    Z: float
+    orbitals: List[I.Orbital]
+    interacting: bool
+    correlation: bool
+
+
+ATOMS = {
+    "H": AtomSpec("H", 1.0, I.ORBITALS_H, False, False),
+    "He": AtomSpec("He", 2.0, I.ORBITALS_HE, True, True),
+    "Ar": AtomSpec("Ar", 18.0, I.ORBITALS_AR, True, True),
+}
+
+
+def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser: LaserSpec,
+                 mask_width: float, zeta: float = 0.5, n_steps: Optional[int] = None,
+                 device: Optional[str] = None, gs_cache: Optional[dict] = None,
+                 W: Optional[np.ndarray] = None) -> RunInputs:
+    """One of the benchmark configurations: sin^2 pulse, cos^(1/8) mask, Z = true nuclear charge.
+
+    Hartree/XC runs use the reference's multipole treatment (L <= 3, N_har = 4) with Slater
+    exchange plus PW92 correlation.
+    """
+    spec = ATOMS[atom]
+    grid = I.make_grid(n_r, r_max, I.zeta_physical_to_ref(zeta, r_max))
+    key = (atom, n_r, r_max)
+    gs = None if gs_cache is None else gs_cache.get(key)
+    if gs is None:
+        gs = I.ground_state(grid, spec.Z, spec.orbitals, interacting=spec.interacting,
+                            correlation=spec.correlation)
+        if gs_cache is not None:
+            gs_cache[key] = gs
+    full = I.steps_for_sin2(dt, laser.omega, laser.cycles)
+    n_t = full if n_steps is None else n_steps
+    E = I.field_sin2(n_t, dt, laser.e0, laser.omega, laser.cycles, laser.cep)
+    target = 0 if not spec.interacting else 1
+    return build_run(grid, l_max + 1, dt, gs, E, absorber="mask", mask_width=mask_width,
+                     n_har=4 if spec.interacting else 2, use_hartree=1 if spec.interacting else 0,
+                     target_id=target, xc_correlation=spec.correlation,
+                     name=f"{atom}-N{n_r}-L{l_max}", omega0=laser.omega, device=device, W=W)
+
+
+def config_hydrogen(n_steps=None, device=None) -> RunInputs:
+    """H FP64: N_r=200, r_max=100, l_max=32, 800 nm, 1e14 W/cm^2, 4-cycle sin^2, dt=0.05, mask 20 a.u."""
+    return baseline_run("H", 200, 100.0, 32, 0.05, LaserSpec(1e14, 800.0, 4.0, 0.0), 20.0,
+                        n_steps=n_steps, device=device)
+
+
+def config_helium(n_steps=None, device=None) -> RunInputs:
+    """He LDA FP64: N_r=400, r_max=200, l_max=64, 800 nm, 1.5e14, 8 cycles, dt=0.03, mask 40 a.u."""
+    return baseline_run("He", 400, 200.0, 64, 0.03, LaserSpec(1.5e14, 800.0, 8.0, 0.0), 40.0,
+                        n_steps=n_steps, device=device)
+
+
+def config_argon(n_steps=None, device=None) -> RunInputs:
+    """Ar LDA: N_r=600, r_max=300, l_max=96, 800 nm, 1.4e14, 10 cycles, dt=0.02, mask 60 a.u."""
+    return baseline_run("Ar", 600, 300.0, 96, 0.02, LaserSpec(1.4e14, 800.0, 10.0, 0.0), 60.0,
+                        n_steps=n_steps, device=device)

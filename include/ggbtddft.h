@@ -1,0 +1,145 @@
+/*
+ * ggbtddft.h -- C ABI of the B200 split-operator time step (libggbtddft.so).
+ *
+ * Drop-in replacement for the time loop of ggbTDDFT's main.cu: the work of
+ *   h_timePropagation(ksoSetTD, hartree, propagators, mesh, observables, temp, handles, scandx)
+ *   (src/subFunctions/timePropagation/h_timePropagation.cuh:32-114)
+ * together with the loaders it depends on (src/main.cu:442-481).  The reference has no plugin or
+ * FFI interface: its seam is that function plus its workingData files, configured by compile-time
+ * macros (src/params.cuh).  Here every size is a run-time value, several independent runs
+ * ("scans", src/main.cu:460) advance together, and every call returns a status code instead of
+ * calling exit() or assert().
+ *
+ * Conventions
+ *  - All pointer arguments may point to host memory (pageable or pinned) or to device memory;
+ *    the library copies through unified addressing.  Inputs are copied in; the context owns all
+ *    device buffers.
+ *  - Complex numbers are interleaved (re, im) doubles, i.e. the layout of the reference's
+ *    double2 / complex128 files.
+ *  - One context per host thread.  All device work of a call is issued on the stream passed in
+ *    (NULL = the legacy default stream); set-up calls are synchronous.
+ *  - Return value 0 = success, < 0 = error (see ggb_status for the message).
+ */
+#ifndef GGBTDDFT_H
+#define GGBTDDFT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ggb_ctx ggb_ctx;
+
+/* precision of the step (radial propagator and angular transforms) */
+enum {
+  GGB_FP64 = 0,        /* complex128 orbitals, FP64 arithmetic: parity form                         */
+  GGB_SPLIT_BF16 = 1,  /* complex64 orbitals, 3xBF16 split products on tcgen05, FP32 accumulation    */
+  GGB_SPLIT_TF32 = 2   /* complex64 orbitals, 3xTF32 split products on tcgen05, FP32 accumulation    */
+};
+
+/* angular couplings (workingData/hamiltonian/propagatorsL/<dir>):  P 001/001, FP 001/003,
+   D 002/002, FF 003/003 (h_initialisePropagators.cuh:26-117) */
+enum { GGB_COUPLING_P = 0, GGB_COUPLING_FP = 1, GGB_COUPLING_D = 2, GGB_COUPLING_FF = 3 };
+
+/* run flags */
+enum {
+  GGB_RUN_XC_PW92 = 1   /* add PW92 correlation to the TD exchange potential (not in the reference) */
+};
+
+/* error codes */
+enum {
+  GGB_OK = 0,
+  GGB_ERR_ARG = -1,       /* invalid argument / size                       */
+  GGB_ERR_CUDA = -2,      /* a CUDA runtime call failed                     */
+  GGB_ERR_STATE = -3,     /* call out of order (e.g. step before set-up)    */
+  GGB_ERR_DEVICE = -4,    /* sticky device status set (NaN, norm growth, step overflow) */
+  GGB_ERR_NOMEM = -5      /* device allocation failed                      */
+};
+
+/* A grid group: runs that share the radial grid, N_l and the radial propagators W_l. */
+typedef struct ggb_group_desc {
+  int n_r;      /* radial points N_r (any value >= 2; no multiple-of-32 restriction)       */
+  int n_l;      /* angular momenta N_l = l_max + 1 (<= 256)                                 */
+  int n_m;      /* number of azimuthal blocks N_m (m = 0 .. n_m-1)                          */
+} ggb_group_desc;
+
+/* One atom-in-field run (one "scan" of the reference). */
+typedef struct ggb_run_desc {
+  int group;        /* index of its grid group                                             */
+  int n_orb;        /* active Kohn-Sham orbitals N_kso                                      */
+  int n_har;        /* N_har: number of Hartree multipoles (params.cuh:55)                  */
+  int use_hartree;  /* USE_HARTREE (params.cuh:56)                                          */
+  int target_id;    /* targetID (params.cuh:36); > 0 enables the interacting couplings      */
+  int flags;        /* GGB_RUN_*                                                            */
+  double dt;        /* time step (a.u.)                                                     */
+} ggb_run_desc;
+
+typedef struct ggb_dims {
+  int n_groups;
+  int n_runs;
+  int precision;    /* GGB_FP64 / GGB_SPLIT_BF16 / GGB_SPLIT_TF32                           */
+  int n_t;          /* capacity of every run's field and observable time series             */
+  int per_l;        /* 1: keep dipole/acceleration per (l, orbital) as the reference does   */
+} ggb_dims;
+
+/* Create a context.  Replaces the allocations of src/main.cu:228-423. */
+int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run_desc* runs,
+               ggb_ctx** out);
+
+/* Radial grid of a group: r, drdx = dr/dx and P = P_{N_g}(x) (workingData/mesh/{r,drdx,P}.bin;
+   h_initialiseMesh.cuh:1-81). */
+int ggb_set_grid(ggb_ctx* ctx, int group, const double* r, const double* drdx, const double* P,
+                 int n_r);
+
+/* Radial propagators W[l][a][b], complex128, the propagatorL%03d.bin layout
+   (h_initialisePropagators.cuh:12-22).  Applied as x_l <- A x_l with A(a,b) = W[l][b][a],
+   i.e. the column-major reading of cublasZgemmBatched in h_propagationH0
+   (h_timePropagation.cuh:1-30). */
+int ggb_set_radial_propagators(ggb_ctx* ctx, int group, const double* W);
+
+/* Eigen-system of one angular coupling for one m: V[l][j] (N_l x N_l) and D[j] (N_l), the
+   V%03d.bin / D%03d.bin files (h_initialisePropagators.cuh:26-117). */
+int ggb_set_angular(ggb_ctx* ctx, int group, int coupling, int m, const double* V, const double* D);
+
+/* Initial orbitals x[l][kso][r] (complex128), and l, m, occupation per orbital, frozen density
+   (h_initialiseTDKSOSet.cuh:19-107).  Resets the run's step counter and observables. */
+int ggb_set_orbitals(ggb_ctx* ctx, int run, const double* x, const int* l, const int* m,
+                     const int* occ, const double* rho_frozen);
+
+/* Laser field E[t] of a run, n_t values (h_initialiseField.cuh:1-40). */
+int ggb_set_field(ggb_ctx* ctx, int run, const double* E, int n_t);
+
+/* Advance every run by n_steps steps, asynchronously on `stream` (a cudaStream_t).
+   The first call after ggb_set_orbitals computes the initial potentials
+   (h_timePropagation.cuh:47-57).  Replays one captured CUDA graph per chunk of steps. */
+int ggb_step(ggb_ctx* ctx, int n_steps, void* stream);
+
+/* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */
+int ggb_get_step(ggb_ctx* ctx, int* step);
+
+/* Observables of a run for steps [0, n_steps): dip/acc are complex128.
+   per_l = 1: dip[l][kso][t] as h_dipoleMoment (main.cu:395); requires ggb_dims.per_l.
+   per_l = 0: dip[kso][t] = sum over l.   norm[kso][t] = sum_l sum_r |x|^2 (not in the reference).
+   Any output pointer may be NULL.  Synchronises the context's work. */
+int ggb_get_observables(ggb_ctx* ctx, int run, double* dip, double* acc, double* norm, int per_l,
+                        int n_steps);
+
+/* Current orbitals x[l][kso][r] of a run (complex128). */
+int ggb_get_orbitals(ggb_ctx* ctx, int run, double* x);
+
+/* Current potentials of a run: v[L][r] (L < 4), v0[r], vexc[r], vexc0[r]; any may be NULL. */
+int ggb_get_potentials(ggb_ctx* ctx, int run, double* v, double* v0, double* vexc, double* vexc0);
+
+/* Sticky device status word (bit 0 NaN/Inf, bit 1 step beyond n_t, bit 2 norm growth) and the
+   last error message.  Returns the status word (>= 0) or an error code. */
+int ggb_status(ggb_ctx* ctx, char* msg, int len);
+
+/* Release every device buffer of the context. */
+void ggb_destroy(ggb_ctx* ctx);
+
+/* Library version string. */
+const char* ggb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GGBTDDFT_H */

@@ -1,0 +1,77 @@
+"""The oracle against the reference's own outputs and known-answer properties (CPU only)."""
+import os
+
+import numpy as np
+import pytest
+
+from ggbtddft_b200 import inputs as I
+from ggbtddft_b200 import problems as P
+from oracle.step_oracle import propagate
+from tests.helpers import GOLDEN, load_ref_case, rel_err, to_oracle
+
+
+@pytest.mark.parametrize("n", [32, 64, 128, 256, 512, 1024])
+def test_lobatto_nodes_match_shipped_roots(n):
+    ref = np.load(os.path.join(GOLDEN, "lobatto_roots.npz"))[f"n{n}"]
+    assert np.max(np.abs(I.lobatto_interior_nodes(n) - ref)) < 5e-15
+
+
+@pytest.mark.parametrize("case", ["h64", "ne3_64"])
+def test_oracle_matches_reference_binary(case):
+    """Dipole series of the reference main.cu (sm_100a build, same inputs) vs the oracle."""
+    run, dref = load_ref_case(case)
+    out = propagate(to_oracle(run))
+    assert out["dipole"].shape == dref.shape
+    assert rel_err(out["dipole"], dref) < 1e-10
+    assert rel_err(out["dipole"].sum(axis=0), dref.sum(axis=0)) < 1e-10
+
+
+def test_p_eigenvalues_are_gauss_legendre_nodes():
+    V, D = I.angular_eigensystems(12, 1)["P"]
+    nodes, _ = np.polynomial.legendre.leggauss(12)
+    assert np.allclose(np.sort(D[0]), np.sort(nodes), atol=1e-14)
+
+
+@pytest.mark.parametrize("coupling", I.COUPLINGS)
+def test_angular_eigenvectors_orthogonal(coupling):
+    V, D = I.angular_eigensystems(20, 3)[coupling]
+    for m in range(3):
+        B = V[m][m:, m:]
+        assert np.allclose(B.T @ B, np.eye(20 - m), atol=1e-13)
+        assert np.all(V[m][:m] == 0) and np.all(V[m][:, :m] == 0)
+
+
+def test_radial_propagator_unitary_without_absorber():
+    grid = I.make_grid(32, 30.0, 1.0)
+    gs = I.ground_state(grid, 1.0, I.ORBITALS_H, interacting=False)
+    W = I.radial_propagators(grid, 3, 0.05, gs.v_ion.astype(complex), gs.vscf, np.zeros(32))
+    for l in range(3):
+        s = np.linalg.svd(W[l], compute_uv=False)
+        assert np.allclose(s, 1.0, atol=1e-12)
+        assert np.allclose(W[l], W[l].T, atol=1e-13)  # complex-symmetric
+
+
+def test_field_free_ground_state_is_stationary():
+    run = P.reference_like(32, 8, 20, "H", intensity=1e-30)
+    run = run.with_field(np.zeros(20))
+    out = propagate(to_oracle(run))
+    x0 = run.x0[0, 0]
+    x = out["x"][0, 0]
+    # |x(t)| unchanged away from the absorber, phase exp(-i e t)
+    inner = run.grid.r < 10.0
+    assert np.allclose(np.abs(x[inner]), np.abs(x0[inner]), atol=1e-6)
+
+
+def test_oracle_quirk_tail_loop_of_octupole_density():
+    """hartreePotentialDensity.cuh:150 restarts the L=3 tail loop at N_l-4: that l counts twice."""
+    from oracle.step_oracle import OracleState
+    run = P.reference_like(32, 10, 4, "Ne3", perturb=0.1)
+    st = OracleState(to_oracle(run))
+    x = np.zeros_like(run.x0)
+    x[6, 0, :] = 1.0        # l = N_l - 4
+    x[3, 0, :] = 1.0        # l - 3
+    d = st.density_multipoles(x)[3]
+    from oracle.step_oracle import f3lm
+    # f3lm(3) x3.x6 is counted by the l=3 up-term, the middle loop's l=6 down-term and the tail's
+    expect = float(run.occ[0]) * 3 * f3lm(3, 0)
+    assert np.allclose(d, expect)
