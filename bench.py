@@ -1,0 +1,327 @@
+"""Throughput of the split-operator time step on B200: orbital-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+A "step" is one time step of every run of the workload (both angular half-steps, the radial
+propagator, density, Hartree/exchange potentials and the dipole/acceleration/norm reductions).
+``value`` = sum over runs of (orbitals x steps) / device time of the K timed steps, all inputs
+resident in HBM, steps replayed from a captured CUDA graph.  ``e2e`` is the same metric through
+the C ABI from host buffers: orbitals and field uploaded, K steps, per-l dipole/acceleration and
+norm series downloaded, wall clock.
+
+Multi-GPU (torchrun): every rank runs an independent replica of the workload (the runs of an
+ensemble are independent; there is no exchange step), ``value`` = all ranks' orbital-steps / the
+slowest rank's device time.
+
+``--impl reference`` times the reference algorithm on the host CPU: the FP64 NumPy restatement of
+the reference time loop (``oracle/step_oracle.py``; the reference itself is a CUDA program with no
+CPU path), on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+# ---------------------------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------------------------
+
+def workload_runs(name: str, n_t: int, device=None):
+    """Return (runs, precision, description dict)."""
+    from ggbtddft_b200 import problems as P
+    if name == "ar-fp64":
+        run = P.config_argon(n_steps=n_t, device=device)
+        return [run], "fp64", dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02, "
+                                            "800 nm 1.4e14 W/cm^2 10-cycle sin^2 (first steps of the pulse)",
+                                   runs=1, n_r=600, l_max=96, n_orb=9, precision="fp64")
+    if name == "he-fp64":
+        run = P.config_helium(n_steps=n_t, device=device)
+        return [run], "fp64", dict(workload="He LDA, 1 orbital, N_r=400, r_max=200, l_max=64, dt=0.03",
+                                   runs=1, n_r=400, l_max=64, n_orb=1, precision="fp64")
+    if name == "h-fp64":
+        run = P.config_hydrogen(n_steps=n_t, device=device)
+        return [run], "fp64", dict(workload="H, 1 orbital, N_r=200, r_max=100, l_max=32, dt=0.05",
+                                   runs=1, n_r=200, l_max=32, n_orb=1, precision="fp64")
+    raise SystemExit(f"unknown workload {name}")
+
+
+DEFAULT_WORKLOAD = "ar-fp64"
+
+
+# ---------------------------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------------------------
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def kernel_traffic(run, precision):
+    """Algorithmic bytes and flops of each phase of one step for one run."""
+    n_r, n_l, n_orb = run.n_r, run.n_l, run.n_orb
+    cb = 16 if precision == "fp64" else 8          # bytes per complex orbital entry
+    wb = 16 if precision == "fp64" else 8          # bytes per complex W entry (FP64 / split hi+lo)
+    x = cb * n_r * n_l * n_orb
+    n_ops_half = 1 + (4 if (run.use_hartree and run.target_id > 0 and run.n_har >= 4) else 1)
+    ang_flops = n_ops_half * 4.0 * n_l * n_l * n_r * n_orb   # real x complex MACs = 4 flop
+    return {
+        "radial": dict(bytes=wb * n_r * n_r * n_l + 2 * x, flops=8.0 * n_r * n_r * n_l * n_orb),
+        "angular_first": dict(bytes=2 * x, flops=ang_flops),
+        "angular_second": dict(bytes=2 * x, flops=ang_flops),
+    }
+
+
+# ---------------------------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------------------------
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from ggbtddft_b200.engine import TimePropagation
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    n_t = args.warmup + args.steps + 8
+    runs, precision, desc = workload_runs(args.workload, n_t, device="cuda")
+    units_per_step = sum(r.n_orb for r in runs)
+    tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
+    stream = torch.cuda.Stream()
+    h = stream.cuda_stream
+    hbm_peak, _, peak_kind = read_peaks()
+
+    # warm-up (also captures the step graph)
+    tp.step(args.warmup, h)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        tp.step(args.steps, h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st, msg = tp.status()
+    if st != 0:
+        raise SystemExit(f"device status {st}: {msg}")
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * units_per_step * args.steps / (ms_max / 1e3)
+
+    # per-kernel durations (each phase launched alone, CUDA events on the launching stream)
+    reps = 20
+    phase_ms = {}
+    for ph, name in ((1, "radial"), (0, "angular_first"), (2, "angular_second"), (3, "finalize")):
+        tp.launch_phase(ph, h)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            tp.launch_phase(ph, h)
+        b.record(stream)
+        torch.cuda.synchronize()
+        phase_ms[name] = a.elapsed_time(b) / reps
+    tp.close()
+
+    # end to end through the C ABI from host buffers
+    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
+    tp2.step(args.warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = 0
+    for i, r in enumerate(runs):
+        tp2.set_orbitals(i, r.x0)
+        tp2.set_field(i, r.E)
+        h2d += r.x0.nbytes + r.E.nbytes
+    tp2.step(args.steps)
+    d2h = 0
+    for i in range(len(runs)):
+        o = tp2.observables(i, per_l=True, n_steps=args.steps)
+        d2h += o["dipole"].nbytes + o["acceleration"].nbytes + o["norm"].nbytes
+    e2e_s = time.perf_counter() - t0
+    tp2.close()
+    e2e_value = world * units_per_step * args.steps / e2e_s
+
+    # roofline of the dominant kernel
+    tr = {k: sum(kernel_traffic(r, precision)[k]["bytes"] for r in runs) for k in ("radial", "angular_first", "angular_second")}
+    fl = {k: sum(kernel_traffic(r, precision)[k]["flops"] for r in runs) for k in ("radial", "angular_first", "angular_second")}
+    dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
+    kernels = {}
+    for k in ("radial", "angular_first", "angular_second"):
+        gbs = tr[k] / (phase_ms[k] / 1e3) / 1e9
+        kernels[k] = dict(ms=round(phase_ms[k], 5), algorithmic_bytes=tr[k], gbs=round(gbs, 1),
+                          tflops=round(fl[k] / (phase_ms[k] / 1e3) / 1e12, 3))
+    kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
+    achieved = tr["radial"] / (phase_ms["radial"] / 1e3) / 1e9
+    roofline = dict(bound="hbm", kernel="radial propagator (k_radial_fp64)", achieved=round(achieved, 1),
+                    peak=hbm_peak, unit="GB/s", frac=round(achieved / hbm_peak, 4), traffic=None,
+                    peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom, kernels=kernels)
+    return dict(value=value, ms=ms_max, units_per_step=units_per_step, desc=desc, precision=precision,
+                clocks=clk.summary(), roofline=roofline,
+                e2e=dict(value=e2e_value, unit="orbital-steps/s", h2d_bytes_per_step=int(h2d / args.steps),
+                         d2h_bytes_per_step=int(d2h / args.steps)),
+                gpu_launches=4 * args.steps * len(tp.groups))
+
+
+def cpu_port_rate(runs, n_steps: int, warmup: int = 1):
+    """Orbital-steps/s of the CPU oracle on ``n_steps`` steps of the first run."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle.step_oracle import OracleProblem, OracleState
+    r = runs[0]
+    prob = OracleProblem(r=r.grid.r, drdx=r.grid.drdx, P=r.grid.P, W=r.W, V=r.V, D=r.D, x0=r.x0, m=r.m_active,
+                         occ=r.occ, rho_frozen=r.rho_frozen, E=r.E, dt=r.dt, n_har=r.n_har,
+                         use_hartree=r.use_hartree, target_id=r.target_id, xc_correlation=r.xc_correlation)
+    st = OracleState(prob)
+    st.init_potentials()
+    for t in range(warmup):
+        st.step(t)
+    t0 = time.perf_counter()
+    for t in range(warmup, warmup + n_steps):
+        st.step(t)
+    dt = time.perf_counter() - t0
+    return r.n_orb * n_steps / dt, dt
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the oracle (FP64 NumPy restatement of the reference loop) on the host cores."""
+    if rank != 0:
+        return None
+    n_t = args.warmup + args.steps + 8
+    runs, precision, desc = workload_runs(args.workload, n_t)
+    rate, dt = cpu_port_rate(runs, args.steps, warmup=args.warmup)
+    return dict(value=rate, desc=desc, seconds=dt, sample=f"run 0 of {len(runs)}, {args.steps} steps")
+
+
+# ---------------------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=40)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = world > 1
+    metric = "orbital-steps/s (batched time step, one B200)"
+    cores = os.cpu_count()
+
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if rank == 0:
+            line = dict(metric=metric, value=res["value"], unit="orbital-steps/s", n_gpus=args.gpus,
+                        steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * res["seconds"] / args.steps,
+                        higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                        data="synthetic (seeded laser parameters; LDA ground state computed at set-up)",
+                        config=dict(res["desc"], l2="n/a (CPU)"), impl="reference",
+                        cpu_baseline=dict(value=res["value"], unit="orbital-steps/s", cores=cores, kind="port",
+                                          sample=res["sample"]),
+                        e2e=dict(value=res["value"], unit="orbital-steps/s", h2d_bytes_per_step=0,
+                                 d2h_bytes_per_step=0))
+            print(json.dumps(line))
+        return
+
+    import torch
+    if dist:
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = run_ours(args, rank, world, dist)
+    cpu = None
+    if rank == 0 and world == 1:
+        n_t = args.cpu_sample_steps + 4
+        runs, _, _ = workload_runs(args.workload, n_t)
+        rate, dt = cpu_port_rate(runs, args.cpu_sample_steps)
+        cpu = dict(value=rate, unit="orbital-steps/s", cores=cores, kind="port",
+                   sample=f"oracle (FP64 NumPy restatement of the reference loop), run 0 of {len(runs)}, "
+                          f"{args.cpu_sample_steps} steps, {dt:.1f} s")
+    if rank == 0:
+        desc = dict(res["desc"])
+        desc["l2"] = "inputs larger than L2 (radial propagators stream from HBM every step)"
+        desc["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+        line = dict(metric=metric, value=res["value"], unit="orbital-steps/s", n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=res["ms"] / args.steps, higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f64" if res["precision"] == "fp64" else "f32+split-bf16",
+                    data="synthetic (seeded laser parameters; LDA ground state computed at set-up)", config=desc,
+                    roofline=res["roofline"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
+                    gpu_launches=res["gpu_launches"])
+        print(json.dumps(line))
+    if dist:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,133 @@
+// Epilogue helpers shared by the angular kernels of both forms: density multipoles and
+// dipole/acceleration partial sums of one orbital column over one tile of radii.  The shared-memory
+// orbitals may be complex128 (FP64 form) or complex64 (split form); products and sums are FP64.
+#pragma once
+#include "ggb_internal.cuh"
+
+namespace ggb {
+
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+__device__ __forceinline__ double cf(const double* tab, int n_l, int l) {
+  return (l >= 0 && l < n_l) ? tab[l] : 0.0;
+}
+
+template <class C>
+__device__ __forceinline__ double xdot(const C* xs, int n_l, int a, int b, int lane) {
+  if (a < 0 || a >= n_l || b < 0 || b >= n_l) return 0.0;
+  const C xa = xs[a * TR + lane];
+  const C xb = xs[b * TR + lane];
+  return (double)xa.x * (double)xb.x + (double)xa.y * (double)xb.y;
+}
+
+// One multipole of one orbital's density at one radius, with the reference's literal l ranges
+// (hartreePotentialDensity.cuh:21-177, including the tail loop of L = 3 that restarts at N_l-4).
+template <class C>
+__device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane,
+                                    const double* coef, int n_m) {
+  const double* cu = coef + ((size_t)CF_CU * n_m + m) * n_l;
+  const double* cd = coef + ((size_t)CF_CD * n_m + m) * n_l;
+  const double* pp = coef + ((size_t)CF_P * n_m + m) * n_l;
+  const double* qu = coef + ((size_t)CF_QU * n_m + m) * n_l;
+  const double* qd = coef + ((size_t)CF_QD * n_m + m) * n_l;
+  const double* p3 = coef + ((size_t)CF_P3 * n_m + m) * n_l;
+  const double* f3 = coef + ((size_t)CF_F3 * n_m + m) * n_l;
+  double d = 0.0;
+  if (L == 0) {
+    for (int lp = m; lp < n_l; ++lp) {
+      const C v = xs[lp * TR + lane];
+      d += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+    }
+  } else if (L == 1) {
+    int lp = m;
+    d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
+    for (lp = m + 1; lp < n_l - 1; ++lp)
+      d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+    lp = n_l - 1;
+    d += cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+  } else if (L == 2) {
+    for (int lp = m; lp < m + 2; ++lp)
+      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+    for (int lp = m + 2; lp < n_l - 2; ++lp)
+      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) +
+           cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+    for (int lp = n_l - 2; lp < n_l; ++lp)
+      d += cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+  } else if (L == 3) {
+    int lp = m;
+    d += cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = m + 1; lp < m + 3; ++lp)
+      d += cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) + cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) +
+           cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = m + 3; lp < n_l - 3; ++lp)
+      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    for (lp = n_l - 4; lp < n_l - 1; ++lp)
+      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
+    d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane);
+  }
+  return d;
+}
+
+__device__ __forceinline__ dd warp_sum_dd(double v) {
+  dd a{v, 0.0};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const dd b{__shfl_xor_sync(0xffffffffu, a.hi, o), __shfl_xor_sync(0xffffffffu, a.lo, o)};
+    a = dd_add(a, b);
+  }
+  return a;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Dipole and acceleration partial sums over this tile's radii for every l of one column
+// (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc).
+template <class C>
+__device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m, int tile, int lane,
+                                 int warp, double rr, double fr2) {
+  const int n_l = g.n_l;
+  const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
+  const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
+  for (int l = warp; l < n_l; l += ANG_WARPS) {
+    double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (l >= m) {
+      const double2 xl = to_d2(xs[l * TR + lane]);
+      const double2 xu = (l + 1 < n_l) ? to_d2(xs[(l + 1) * TR + lane]) : make_double2(0.0, 0.0);
+      const double2 xd = (l >= 1) ? to_d2(xs[(l - 1) * TR + lane]) : make_double2(0.0, 0.0);
+      const double c_u = cu[l], c_d = cd[l];
+      double2 z1, z2;
+      if (l == m) {
+        z1 = make_double2(rr * c_u * xu.x, rr * c_u * xu.y);
+        z2 = make_double2(fr2 * c_u * xu.x, fr2 * c_u * xu.y);
+      } else if (l == n_l - 1) {
+        z1 = make_double2(rr * c_d * xd.x, rr * c_d * xd.y);
+        z2 = make_double2(fr2 * c_d * xd.x, fr2 * c_d * xd.y);
+      } else {
+        z1 = make_double2(rr * c_u * xu.x + rr * c_d * xd.x, rr * c_u * xu.y + rr * c_d * xd.y);
+        z2 = make_double2(fr2 * (c_u * xu.x + c_d * xd.x), fr2 * (c_u * xu.y + c_d * xd.y));
+      }
+      // conj(x_l) . z
+      out.x = xl.x * z1.x + xl.y * z1.y;
+      out.y = xl.x * z1.y - xl.y * z1.x;
+      out.z = xl.x * z2.x + xl.y * z2.y;
+      out.w = xl.x * z2.y - xl.y * z2.x;
+    }
+    // compensated (double-double) reduction over the tile's radii
+    const dd sx = warp_sum_dd(out.x), sy = warp_sum_dd(out.y), sz = warp_sum_dd(out.z), sw = warp_sum_dd(out.w);
+    if (lane == 0) {
+      double4* o = g.obs + 2 * (((size_t)col * n_l + l) * g.n_tiles + tile);
+      o[0] = make_double4(sx.hi, sy.hi, sz.hi, sw.hi);
+      o[1] = make_double4(sx.lo, sy.lo, sz.lo, sw.lo);
+    }
+  }
+}
+
+
+}  // namespace ggb

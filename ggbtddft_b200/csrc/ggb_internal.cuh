@@ -10,7 +10,8 @@
 //   dph      angular eigenvalues D[c][m][j], [4][N_m][ldS].
 //   coef     angular coefficient tables [COEF_N][N_m][N_l] (cu, cd, p, qu, qd, p3lm, f3lm).
 //   dens     density partials per column [n_cols][4][N_r] (not yet occupation weighted).
-//   obs      dipole/acceleration partials per column, l and r-tile [n_cols][N_l][n_tiles] double4.
+//   obs      dipole/acceleration partials per column, l and r-tile [n_cols][N_l][n_tiles][2] double4
+//            (double-double: high parts, then low parts).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -19,7 +20,8 @@ namespace ggb {
 
 constexpr int TR = 32;            // radii per angular tile (one warp-width, coalesced along r)
 constexpr int ANG_WARPS = 8;      // warps per angular CTA
-constexpr int MAX_NL = 256;       // largest N_l supported by the angular kernels
+constexpr int MAX_NL = 220;       // largest N_l: two [N_l][32] complex128 tiles fit in 227 KB of shared memory
+constexpr int MAX_NR = 8192;      // largest N_r: three [N_r] FP64 rows of the potentials kernel
 constexpr int N_DEN = 4;          // density multipoles carried per column (L = 0..3)
 
 // status bits (sticky, OR-ed on the device)
@@ -87,7 +89,7 @@ struct GroupArgs {
   int* step;                // ctx-wide step counter
   unsigned* status;
   unsigned* done;           // block counter for the last-block step increment
-  Chain chain[2];
+  Chain chain[3];   // first half, second half, empty (initial partials)
 };
 
 __device__ __forceinline__ double2 cmul_conj_phase(double2 x, double eta) {
@@ -120,5 +122,7 @@ void launch_radial_fp64(const GroupArgs& g, const double2* W, const double2* xin
                         cudaStream_t s);
 void launch_finalize(const GroupArgs& g, int mode, cudaStream_t s);
 size_t angular_smem_fp64(int n_l);
+cudaError_t configure_kernels_fp64(int n_l_max, int n_r_max);
+cudaError_t set_max_dynamic_smem(const void* fn, int optin);
 
 }  // namespace ggb

@@ -17,117 +17,13 @@
 //                  (h_calculateExchangeCorrelationPotential.cuh:1-56), step counter.
 #include <cstdio>
 #include "ggb_internal.cuh"
+#include "ggb_angular.cuh"
 
 namespace ggb {
 
 // ---------------------------------------------------------------------------------------------
 // angular chain
 // ---------------------------------------------------------------------------------------------
-
-__device__ __forceinline__ double cf(const double* tab, int n_l, int l) {
-  return (l >= 0 && l < n_l) ? tab[l] : 0.0;
-}
-
-__device__ __forceinline__ double xdot(const double2* xs, int n_l, int a, int b, int lane) {
-  if (a < 0 || a >= n_l || b < 0 || b >= n_l) return 0.0;
-  const double2 xa = xs[a * TR + lane];
-  const double2 xb = xs[b * TR + lane];
-  return xa.x * xb.x + xa.y * xb.y;
-}
-
-// One multipole of one orbital's density at one radius, with the reference's literal l ranges
-// (hartreePotentialDensity.cuh:21-177, including the tail loop of L = 3 that restarts at N_l-4).
-__device__ double density_multipole(int L, int m, int n_l, const double2* xs, int lane,
-                                    const double* coef, int n_m) {
-  const double* cu = coef + ((size_t)CF_CU * n_m + m) * n_l;
-  const double* cd = coef + ((size_t)CF_CD * n_m + m) * n_l;
-  const double* pp = coef + ((size_t)CF_P * n_m + m) * n_l;
-  const double* qu = coef + ((size_t)CF_QU * n_m + m) * n_l;
-  const double* qd = coef + ((size_t)CF_QD * n_m + m) * n_l;
-  const double* p3 = coef + ((size_t)CF_P3 * n_m + m) * n_l;
-  const double* f3 = coef + ((size_t)CF_F3 * n_m + m) * n_l;
-  double d = 0.0;
-  if (L == 0) {
-    for (int lp = m; lp < n_l; ++lp) {
-      const double2 v = xs[lp * TR + lane];
-      d += v.x * v.x + v.y * v.y;
-    }
-  } else if (L == 1) {
-    int lp = m;
-    d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
-    for (lp = m + 1; lp < n_l - 1; ++lp)
-      d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
-    lp = n_l - 1;
-    d += cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
-  } else if (L == 2) {
-    for (int lp = m; lp < m + 2; ++lp)
-      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
-    for (int lp = m + 2; lp < n_l - 2; ++lp)
-      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) +
-           cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
-    for (int lp = n_l - 2; lp < n_l; ++lp)
-      d += cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
-  } else if (L == 3) {
-    int lp = m;
-    d += cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
-    for (lp = m + 1; lp < m + 3; ++lp)
-      d += cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) + cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) +
-           cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
-    for (lp = m + 3; lp < n_l - 3; ++lp)
-      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
-           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
-    for (lp = n_l - 4; lp < n_l - 1; ++lp)
-      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
-           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
-    d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane);
-  }
-  return d;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Dipole and acceleration partial sums over this tile's radii for every l of one column
-// (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc).
-__device__ void observables_tile(const GroupArgs& g, const double2* xs, int col, int m, int tile, int lane,
-                                 int warp, double rr, double fr2) {
-  const int n_l = g.n_l;
-  const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
-  const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
-  for (int l = warp; l < n_l; l += ANG_WARPS) {
-    double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (l >= m) {
-      const double2 xl = xs[l * TR + lane];
-      const double2 xu = (l + 1 < n_l) ? xs[(l + 1) * TR + lane] : make_double2(0.0, 0.0);
-      const double2 xd = (l >= 1) ? xs[(l - 1) * TR + lane] : make_double2(0.0, 0.0);
-      const double c_u = cu[l], c_d = cd[l];
-      double2 z1, z2;
-      if (l == m) {
-        z1 = make_double2(rr * c_u * xu.x, rr * c_u * xu.y);
-        z2 = make_double2(fr2 * c_u * xu.x, fr2 * c_u * xu.y);
-      } else if (l == n_l - 1) {
-        z1 = make_double2(rr * c_d * xd.x, rr * c_d * xd.y);
-        z2 = make_double2(fr2 * c_d * xd.x, fr2 * c_d * xd.y);
-      } else {
-        z1 = make_double2(rr * c_u * xu.x + rr * c_d * xd.x, rr * c_u * xu.y + rr * c_d * xd.y);
-        z2 = make_double2(fr2 * (c_u * xu.x + c_d * xd.x), fr2 * (c_u * xu.y + c_d * xd.y));
-      }
-      // conj(x_l) . z
-      out.x = xl.x * z1.x + xl.y * z1.y;
-      out.y = xl.x * z1.y - xl.y * z1.x;
-      out.z = xl.x * z2.x + xl.y * z2.y;
-      out.w = xl.x * z2.y - xl.y * z2.x;
-    }
-    out.x = warp_sum(out.x);
-    out.y = warp_sum(out.y);
-    out.z = warp_sum(out.z);
-    out.w = warp_sum(out.w);
-    if (lane == 0) g.obs[((size_t)col * n_l + l) * g.n_tiles + tile] = out;
-  }
-}
 
 constexpr int ANG_JB = 8;   // eigen-channels j per register block
 
@@ -245,7 +141,6 @@ void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, doubl
                          cudaStream_t s) {
   const dim3 grid(g.n_cols * g.n_tiles), block(ANG_WARPS * 32);
   const size_t smem = angular_smem_fp64(g.n_l);
-  cudaFuncSetAttribute(k_angular_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_angular_fp64<<<grid, block, smem, s>>>(g, half, xin, xout, do_obs);
 }
 
@@ -369,6 +264,15 @@ __device__ void block_scan_dd(const double* t, double* out, int n, bool backward
   __syncthreads();
 }
 
+__device__ __forceinline__ dd warp_sum_dd2(dd a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const dd b{__shfl_xor_sync(0xffffffffu, a.hi, o), __shfl_xor_sync(0xffffffffu, a.lo, o)};
+    a = dd_add(a, b);
+  }
+  return a;
+}
+
 __device__ __forceinline__ double ipow(double x, int L) {
   double p = 1.0;
   for (int i = 0; i < L; ++i) p *= x;
@@ -377,7 +281,8 @@ __device__ __forceinline__ double ipow(double x, int L) {
 
 // Blocks: for each run of the group, n_den Hartree blocks (L = 0..n_den-1; block L = 0 also does
 // the exchange potential) + 1 observables block.  mode 0 = initial potentials (no observables,
-// no step increment), mode 1 = end of step.
+// no step increment), mode 1 = end of step, mode 2 = end of step without observables or step
+// increment (profiling).
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode) {
   extern __shared__ double fsm[];  // [3][N_r]
   __shared__ dd wsum[FIN_THREADS / 32];
@@ -395,39 +300,42 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
       if (tid == 0) atomicOr(g.status, ST_STEP_OVERFLOW);
     } else {
       const int n_orb = run.n_orb;
-      // per (l, orbital): sum over r tiles
+      // per (l, orbital): compensated sum over r tiles
       for (int idx = tid; idx < n_l * n_orb; idx += FIN_THREADS) {
         const int l = idx / n_orb, k = idx - l * n_orb;
-        const double4* p = g.obs + ((size_t)(run.col0 + k) * n_l + l) * g.n_tiles;
-        double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+        const double4* p = g.obs + 2 * (((size_t)(run.col0 + k) * n_l + l) * g.n_tiles);
+        dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
         for (int t = 0; t < g.n_tiles; ++t) {
-          const double4 v = p[t];
-          s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+          const double4 h = p[2 * t], lo = p[2 * t + 1];
+          sx = dd_add(sx, dd{h.x, lo.x}); sy = dd_add(sy, dd{h.y, lo.y});
+          sz = dd_add(sz, dd{h.z, lo.z}); sw = dd_add(sw, dd{h.w, lo.w});
         }
         if (g.per_l) {
-          run.dip[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(s.x, s.y);
-          run.acc[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(s.z, s.w);
+          run.dip[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
+          run.acc[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
         }
       }
       // per orbital: totals over l and the norm; one warp per orbital
       const int lane = tid & 31, warp = tid >> 5;
       for (int k = warp; k < n_orb; k += FIN_THREADS / 32) {
-        const double4* p = g.obs + (size_t)(run.col0 + k) * n_l * g.n_tiles;
-        double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+        const double4* p = g.obs + 2 * ((size_t)(run.col0 + k) * n_l * g.n_tiles);
+        dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
         for (int q = lane; q < n_l * g.n_tiles; q += 32) {
-          const double4 v = p[q];
-          s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+          const double4 h = p[2 * q], lo = p[2 * q + 1];
+          sx = dd_add(sx, dd{h.x, lo.x}); sy = dd_add(sy, dd{h.y, lo.y});
+          sz = dd_add(sz, dd{h.z, lo.z}); sw = dd_add(sw, dd{h.w, lo.w});
         }
-        s.x = warp_sum(s.x); s.y = warp_sum(s.y); s.z = warp_sum(s.z); s.w = warp_sum(s.w);
+        sx = warp_sum_dd2(sx); sy = warp_sum_dd2(sy); sz = warp_sum_dd2(sz); sw = warp_sum_dd2(sw);
         const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;  // L = 0 row
-        double nrm = 0.0;
-        for (int q = lane; q < n_r; q += 32) nrm += dn[q];
-        nrm = warp_sum(nrm);
+        dd nd{0.0, 0.0};
+        for (int q = lane; q < n_r; q += 32) nd = dd_add(nd, dd{dn[q], 0.0});
+        nd = warp_sum_dd2(nd);
+        const double nrm = nd.hi + nd.lo;
         if (lane == 0) {
-          run.dip_tot[(size_t)k * run.n_t + step] = make_double2(s.x, s.y);
-          run.acc_tot[(size_t)k * run.n_t + step] = make_double2(s.z, s.w);
+          run.dip_tot[(size_t)k * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
+          run.acc_tot[(size_t)k * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
           run.norm[(size_t)k * run.n_t + step] = nrm;
-          if (!(nrm == nrm) || isinf(nrm) || !(s.x == s.x) || !(s.z == s.z)) atomicOr(g.status, ST_NAN);
+          if (!(nrm == nrm) || isinf(nrm) || !(sx.hi == sx.hi) || !(sz.hi == sz.hi)) atomicOr(g.status, ST_NAN);
           if (nrm > run.norm0[k] * (1.0 + 1e-6) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
         }
       }
@@ -437,10 +345,10 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
     const int lane = tid & 31, warp = tid >> 5;
     for (int k = warp; k < run.n_orb; k += FIN_THREADS / 32) {
       const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;
-      double nrm = 0.0;
-      for (int q = lane; q < n_r; q += 32) nrm += dn[q];
-      nrm = warp_sum(nrm);
-      if (lane == 0) run.norm0[k] = nrm;
+      dd nd{0.0, 0.0};
+      for (int q = lane; q < n_r; q += 32) nd = dd_add(nd, dd{dn[q], 0.0});
+      nd = warp_sum_dd2(nd);
+      if (lane == 0) run.norm0[k] = nd.hi + nd.lo;
     }
   }
 
@@ -536,8 +444,30 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
 void launch_finalize(const GroupArgs& g, int mode, cudaStream_t s) {
   const dim3 grid(g.n_runs * (g.n_den + 1)), block(FIN_THREADS);
   const size_t smem = 3 * (size_t)g.n_r * sizeof(double);
-  cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_finalize<<<grid, block, smem, s>>>(g, mode);
+}
+
+// Allow a kernel the largest dynamic shared memory the device offers beyond its static part.
+cudaError_t set_max_dynamic_smem(const void* fn, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+cudaError_t configure_kernels_fp64(int n_l_max, int n_r_max) {
+  // The attribute is global per function: set it to the device's opt-in maximum once, so that
+  // contexts of different sizes can coexist.  Callers check their own sizes against it.
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (angular_smem_fp64(n_l_max) > (size_t)optin || 3 * (size_t)n_r_max * sizeof(double) > (size_t)optin)
+    return cudaErrorInvalidValue;
+  e = set_max_dynamic_smem((const void*)k_angular_fp64, optin);
+  if (e != cudaSuccess) return e;
+  return set_max_dynamic_smem((const void*)k_finalize, optin);
 }
 
 }  // namespace ggb

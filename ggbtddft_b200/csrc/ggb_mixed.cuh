@@ -1,0 +1,43 @@
+// Split-precision form of the step: complex64 orbitals, radial propagator on tcgen05 tensor
+// cores with 3xBF16 split products and FP32 accumulation in tensor memory, angular chain in FP32,
+// observables and potentials in FP64.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "ggb_internal.cuh"
+
+namespace ggb {
+
+constexpr unsigned ST_TC_TIMEOUT = 8u;   // a bounded wait in a tensor-core kernel gave up
+
+struct MixedGroup {
+  int precision = 0;
+  bool ready = false;
+  int k_pad = 0;        // N_r rounded up to the radial K block (32)
+  int rows_pad = 0;     // N_r rounded up to the radial M tile (128)
+  int bn = 16;          // radial N tile (orbital columns per CTA)
+  int cols_pad = 0;     // n_cols rounded up to the N tile (zero columns keep every TMA box in bounds)
+  int stages = 4;
+  size_t smem = 0;
+  float2* X = nullptr;              // state [N_l][n_cols][N_r]
+  float2* Y = nullptr;              // radial output [N_l][n_cols][N_r]
+  __nv_bfloat16* Xsp = nullptr;     // radial B operand [N_l][4][cols_pad][k_pad]  (re hi, re lo, im hi, im lo)
+  __nv_bfloat16* Wsp = nullptr;     // radial A operand [N_l][4][rows_pad][k_pad] (Wr hi, Wr lo, Wi hi, Wi lo), A(i,k) = W[l][k][i]
+  float* mats_f = nullptr;          // chain matrices in FP32
+  CUtensorMap tmW;
+  CUtensorMap tmX;
+};
+
+int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precision, std::string& err);
+int mixed_load_orbitals(MixedGroup& m, const GroupArgs& a, const double2* x_fp64);
+int mixed_store_orbitals(MixedGroup& m, const GroupArgs& a, double2* x_fp64);
+void mixed_init(MixedGroup& m, const GroupArgs& a, const double2* x_fp64, cudaStream_t s);
+void mixed_step(MixedGroup& m, const GroupArgs& a, cudaStream_t s);
+void mixed_phase(MixedGroup& m, const GroupArgs& a, int phase, cudaStream_t s);
+void mixed_release(MixedGroup& m);
+
+}  // namespace ggb

@@ -113,6 +113,13 @@ int ggb_set_field(ggb_ctx* ctx, int run, const double* E, int n_t);
    (h_timePropagation.cuh:47-57).  Replays one captured CUDA graph per chunk of steps. */
 int ggb_step(ggb_ctx* ctx, int n_steps, void* stream);
 
+/* Profiling hook: launch one phase of the step for every group on `stream`
+   (0 = angular first half, 1 = radial propagator, 2 = angular second half + partial sums,
+   3 = potentials/observables).  It leaves the orbitals in an intermediate state and is meant
+   only for timing a kernel alone; the state must be reset with ggb_set_orbitals afterwards.
+   No counterpart in the reference. */
+int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream);
+
 /* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */
 int ggb_get_step(ggb_ctx* ctx, int* step);
 

@@ -292,6 +292,10 @@ class OracleState:
         n_l = p.n_l
         dip = np.zeros((n_l, p.n_kso), dtype=np.complex128)
         acc = np.zeros((n_l, p.n_kso), dtype=np.complex128)
+        # sum of |terms| of each inner product: the scale that rounding errors of any summation
+        # order (including the reference's cublasZdotc) are proportional to
+        dip_scale = np.zeros((n_l, p.n_kso))
+        acc_scale = np.zeros((n_l, p.n_kso))
         fr2 = np.power(r, -2.0)
         for k in range(p.n_kso):
             m = int(p.m[k])
@@ -311,7 +315,10 @@ class OracleState:
                     z2 = fr2 * (cu * x[l + 1, k] + cd * x[l - 1, k])
                 dip[l, k] = np.vdot(x[l, k], z1)
                 acc[l, k] = np.vdot(x[l, k], z2)
+                dip_scale[l, k] = np.sum(np.abs(x[l, k]) * np.abs(z1))
+                acc_scale[l, k] = np.sum(np.abs(x[l, k]) * np.abs(z2))
         norm = (np.abs(x) ** 2).sum(axis=(0, 2))
+        self.last_scales = (dip_scale, acc_scale)
         return dip, acc, norm
 
     # ----- one step -----
@@ -388,8 +395,9 @@ def propagate(prob: OracleProblem, n_steps: Optional[int] = None):
     """Run the reference time loop for ``n_steps`` steps (default N_t); return the time series.
 
     Returns a dict with ``dipole`` and ``acceleration`` [N_l, N_kso, n_steps] complex (the
-    reference's h_dipoleMoment[l][kso][t] layout), ``norm`` [N_kso, n_steps], the final orbitals
-    ``x`` [N_l, N_kso, N_r] and the final potentials.
+    reference's h_dipoleMoment[l][kso][t] layout), their conditioning scales (sum of |terms| of
+    each inner product), ``norm`` [N_kso, n_steps], the final orbitals ``x`` [N_l, N_kso, N_r]
+    and the final potentials.
     """
     st = OracleState(prob)
     st.init_potentials()
@@ -397,10 +405,14 @@ def propagate(prob: OracleProblem, n_steps: Optional[int] = None):
     dip = np.zeros((prob.n_l, prob.n_kso, n), dtype=np.complex128)
     acc = np.zeros_like(dip)
     norm = np.zeros((prob.n_kso, n))
+    dscale = np.zeros((prob.n_l, prob.n_kso, n))
+    ascale = np.zeros_like(dscale)
     for t in range(n):
         d, a, nm = st.step(t)
         dip[:, :, t] = d
         acc[:, :, t] = a
         norm[:, t] = nm
+        dscale[:, :, t], ascale[:, :, t] = st.last_scales
     return dict(dipole=dip, acceleration=acc, norm=norm, x=st.x, v=st.v, vexc=st.vexc,
-                v0=st.v0, vexc0=st.vexc0, density=st.density)
+                v0=st.v0, vexc0=st.vexc0, density=st.density, dipole_scale=dscale,
+                acceleration_scale=ascale)

@@ -30,3 +30,16 @@ def rel_err(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def obs_close(got, ref, scale, rel=1e-10, cond=1e-13):
+    """|got - ref| <= rel * max|ref| + cond * scale, elementwise.
+
+    ``scale`` is the sum of |terms| of each inner product: per-(l, t) dipole and acceleration sums
+    cancel (terms ~1e-2 summing to ~1e-8 near t = 0), so any two summation orders -- the
+    reference's cublasZdotc included -- differ by ~1e-16 * scale there.
+    """
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    bound = rel * np.abs(ref).max() + cond * np.asarray(scale)
+    return bool(np.all(np.abs(got - ref) <= bound))

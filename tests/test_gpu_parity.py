@@ -1,0 +1,111 @@
+"""Parity of the CUDA path (through the C ABI) with the reference binary's outputs and the oracle."""
+import numpy as np
+import pytest
+
+from ggbtddft_b200 import inputs as I
+from ggbtddft_b200 import problems as P
+from ggbtddft_b200.engine import TimePropagation, h_time_propagation
+from oracle.step_oracle import propagate
+from tests.helpers import load_ref_case, obs_close, rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10   # FP64 form vs the reference / the oracle (relative to the series maximum)
+
+
+@pytest.mark.parametrize("case", ["h64", "ne3_64"])
+def test_fp64_matches_reference_binary(case):
+    run, dref = load_ref_case(case)
+    out = h_time_propagation(run)
+    assert out["dipole"].shape == dref.shape
+    assert rel_err(out["dipole"], dref) < TOL
+    assert rel_err(out["dipole"].sum(axis=0), dref.sum(axis=0)) < TOL
+
+
+def _compare_all(run, n_steps=None):
+    n = run.n_t if n_steps is None else n_steps
+    ref = propagate(to_oracle(run), n)
+    tp = TimePropagation([run])
+    tp.step(n)
+    got = tp.observables(0, per_l=True, n_steps=n)
+    tot = tp.observables(0, per_l=False, n_steps=n)
+    x = tp.orbitals(0)
+    pot = tp.potentials(0)
+    st, msg = tp.status()
+    tp.close()
+    assert st == 0, msg
+    assert obs_close(got["dipole"], ref["dipole"], ref["dipole_scale"], rel=TOL)
+    assert obs_close(got["acceleration"], ref["acceleration"], ref["acceleration_scale"], rel=TOL)
+    assert obs_close(tot["dipole"], ref["dipole"].sum(axis=0), ref["dipole_scale"].sum(axis=0), rel=TOL)
+    assert obs_close(tot["acceleration"], ref["acceleration"].sum(axis=0), ref["acceleration_scale"].sum(axis=0),
+                     rel=TOL)
+    assert rel_err(got["norm"], ref["norm"]) < TOL
+    assert rel_err(x, ref["x"]) < TOL
+    if run.use_hartree and run.target_id > 0:
+        assert rel_err(pot["v"][:run.n_har], ref["v"][:run.n_har]) < TOL
+        assert rel_err(pot["vexc"], ref["vexc"]) < TOL
+        assert rel_err(pot["v0"], ref["v0"]) < TOL
+
+
+@pytest.mark.parametrize("n_r,n_l", [(37, 5), (45, 9), (64, 33)])
+def test_fp64_odd_sizes_hydrogen(n_r, n_l):
+    _compare_all(P.reference_like(n_r, n_l, 24, "H", r_mask=20.0))
+
+
+@pytest.mark.parametrize("n_r,n_l", [(45, 9), (70, 17)])
+def test_fp64_odd_sizes_interacting(n_r, n_l):
+    _compare_all(P.reference_like(n_r, n_l, 20, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=3))
+
+
+def test_fp64_hydrogen_config_shape():
+    """N_r = 200, l_max = 32, sin^2 pulse, cos^(1/8) mask: the hydrogen configuration's sizes."""
+    run = P.config_hydrogen(n_steps=60)
+    _compare_all(run)
+
+
+def test_fp64_pw92_correlation():
+    run = P.reference_like(48, 12, 16, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=5)
+    import dataclasses
+    _compare_all(dataclasses.replace(run, xc_correlation=True))
+
+
+def test_graph_replay_equals_single_steps():
+    run = P.reference_like(64, 16, 80, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=1)
+    a = TimePropagation([run])
+    a.step(70)                     # two graph replays of 32 steps + 6 direct steps
+    b = TimePropagation([run])
+    for _ in range(70):
+        b.step(1)
+    oa, ob = a.observables(0), b.observables(0)
+    assert a.current_step == b.current_step == 70
+    assert np.array_equal(oa["dipole"], ob["dipole"])
+    assert np.array_equal(a.orbitals(0), b.orbitals(0))
+    a.close()
+    b.close()
+
+
+def test_ensemble_group_equals_single_runs():
+    """Three runs sharing one grid group (same W object) with different fields."""
+    base = P.reference_like(64, 16, 30, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=2)
+    t = I.time_grid(30, base.dt)
+    runs = [base.with_field(I.field_super_gaussian(t, e0, 0.057, 150.0, cep))
+            for e0, cep in ((0.05, 0.0), (0.08, 1.0), (0.03, 2.0))]
+    ens = TimePropagation(runs)
+    assert len(ens.groups) == 1
+    ens.step(30)
+    for i, r in enumerate(runs):
+        single = TimePropagation([r])
+        single.step(30)
+        assert rel_err(ens.observables(i)["dipole"], single.observables(0)["dipole"]) < 1e-13
+        single.close()
+    ens.close()
+
+
+def test_step_beyond_field_sets_status_not_fault():
+    run = P.reference_like(32, 8, 4, "H")
+    tp = TimePropagation([run], n_t=4)
+    tp.step(6)
+    st, msg = tp.status()
+    assert st & 2, msg
+    assert "beyond" in msg
+    tp.close()
