@@ -41,6 +41,26 @@ import numpy as np  # noqa: E402
 def workload_runs(name: str, n_t: int, device=None):
     """Return (runs, precision, description dict)."""
     from ggbtddft_b200 import problems as P
+    if name.startswith("ar-ens64"):
+        precision = "fp64" if name.endswith("fp64") else "split_bf16"
+        runs = P.argon_ensemble(64, seed=0, n_steps=n_t, device=device)
+        ladder = ", ".join(f"{g.n_r}/{g.r_max:.0f}/{g.l_max}" for g in P.ARGON_LADDER)
+        return runs, precision, dict(
+            workload="64-run argon LDA in-situ focal scan: I U[0.8,2]e14 W/cm^2, lambda U[800,1300] nm, "
+                     "10-cycle sin^2, dt=0.02, 9 orbitals per run; grids N_r/r_max/l_max on the ladder " + ladder +
+                     " (runs of one grid share W); first steps of the pulse",
+            runs=64, n_orb=9, precision=precision, seed=0)
+    if name.startswith("hhe-ens256"):
+        precision = "fp64" if name.endswith("fp64") else "split_bf16"
+        runs = P.hhe_ensemble(256, seed=0, n_steps=n_t, device=device)
+        return runs, precision, dict(
+            workload="256-run H/He scan: I log-U[0.5,3]e14, CEP U[0,2pi), lambda U[800,1800] nm, 6-cycle sin^2, "
+                     "dt=0.03; grids N_r 200-800, l_max 32-128 on a ladder", runs=256, n_orb=1,
+            precision=precision, seed=0)
+    if name == "ar-split":
+        run = P.config_argon(n_steps=n_t, device=device)
+        return [run], "split_bf16", dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02",
+                                         runs=1, n_r=600, l_max=96, n_orb=9, precision="split_bf16")
     if name == "ar-fp64":
         run = P.config_argon(n_steps=n_t, device=device)
         return [run], "fp64", dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02, "
@@ -57,7 +77,7 @@ def workload_runs(name: str, n_t: int, device=None):
     raise SystemExit(f"unknown workload {name}")
 
 
-DEFAULT_WORKLOAD = "ar-fp64"
+DEFAULT_WORKLOAD = "ar-ens64"
 
 
 # ---------------------------------------------------------------------------------------------
@@ -124,19 +144,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def kernel_traffic(run, precision):
-    """Algorithmic bytes and flops of each phase of one step for one run."""
-    n_r, n_l, n_orb = run.n_r, run.n_l, run.n_orb
-    cb = 16 if precision == "fp64" else 8          # bytes per complex orbital entry
-    wb = 16 if precision == "fp64" else 8          # bytes per complex W entry (FP64 / split hi+lo)
-    x = cb * n_r * n_l * n_orb
-    n_ops_half = 1 + (4 if (run.use_hartree and run.target_id > 0 and run.n_har >= 4) else 1)
-    ang_flops = n_ops_half * 4.0 * n_l * n_l * n_r * n_orb   # real x complex MACs = 4 flop
-    return {
-        "radial": dict(bytes=wb * n_r * n_r * n_l + 2 * x, flops=8.0 * n_r * n_r * n_l * n_orb),
-        "angular_first": dict(bytes=2 * x, flops=ang_flops),
-        "angular_second": dict(bytes=2 * x, flops=ang_flops),
-    }
+def phase_traffic(runs, groups, precision):
+    """Algorithmic bytes and flops of each phase of one step, summed over the grid groups.
+
+    radial: W once per group (16 B per complex FP64, 8 B as split BF16 hi/lo planes) + orbitals in
+    and out; flops 8 N_r^2 N_l per orbital column (the 3x split products are not counted).
+    angular half: orbitals in and out; (#chain GEMMs) x 4 N_l^2 N_r flops per column.
+    """
+    cb = 16 if precision == "fp64" else 8
+    wb = 16 if precision == "fp64" else 8
+    out = {k: dict(bytes=0.0, flops=0.0) for k in ("radial", "angular_first", "angular_second")}
+    for members in groups:
+        r0 = runs[members[0]]
+        n_r, n_l = r0.n_r, r0.n_l
+        cols = sum(runs[i].n_orb for i in members)
+        x = cb * n_r * n_l * cols
+        n_gemm = 2 + (3 if (r0.use_hartree and r0.target_id > 0 and r0.n_har >= 4) else 0)
+        out["radial"]["bytes"] += wb * n_r * n_r * n_l + 2 * x
+        out["radial"]["flops"] += 8.0 * n_r * n_r * n_l * cols
+        for k in ("angular_first", "angular_second"):
+            out[k]["bytes"] += 2 * x
+            out[k]["flops"] += n_gemm * 4.0 * n_l * n_l * n_r * cols
+    return out
 
 
 # ---------------------------------------------------------------------------------------------
@@ -194,43 +223,77 @@ def run_ours(args, rank, world, dist):
     tp.close()
 
     # end to end through the C ABI from host buffers
-    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
-    tp2.step(args.warmup)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    h2d = 0
-    for i, r in enumerate(runs):
-        tp2.set_orbitals(i, r.x0)
-        tp2.set_field(i, r.E)
-        h2d += r.x0.nbytes + r.E.nbytes
-    tp2.step(args.steps)
-    d2h = 0
-    for i in range(len(runs)):
-        o = tp2.observables(i, per_l=True, n_steps=args.steps)
-        d2h += o["dipole"].nbytes + o["acceleration"].nbytes + o["norm"].nbytes
-    e2e_s = time.perf_counter() - t0
-    tp2.close()
-    e2e_value = world * units_per_step * args.steps / e2e_s
+    if not args.e2e:
+        e2e_value, h2d, d2h = None, 0, 0
+    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t) if args.e2e else None
+    if tp2 is not None:
+        tp2.step(args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h2d = 0
+        for i, r in enumerate(runs):
+            tp2.set_orbitals(i, r.x0)
+            tp2.set_field(i, r.E)
+            h2d += r.x0.nbytes + r.E.nbytes
+        tp2.step(args.steps)
+        d2h = 0
+        for i in range(len(runs)):
+            o = tp2.observables(i, per_l=True, n_steps=args.steps)
+            d2h += o["dipole"].nbytes + o["acceleration"].nbytes + o["norm"].nbytes
+        e2e_s = time.perf_counter() - t0
+        tp2.close()
+        e2e_value = world * units_per_step * args.steps / e2e_s
 
     # roofline of the dominant kernel
-    tr = {k: sum(kernel_traffic(r, precision)[k]["bytes"] for r in runs) for k in ("radial", "angular_first", "angular_second")}
-    fl = {k: sum(kernel_traffic(r, precision)[k]["flops"] for r in runs) for k in ("radial", "angular_first", "angular_second")}
+    tf = phase_traffic(runs, tp.groups, precision)
     dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
+    tensor_peak = read_peaks()[1] if precision != "fp64" else None
     kernels = {}
     for k in ("radial", "angular_first", "angular_second"):
-        gbs = tr[k] / (phase_ms[k] / 1e3) / 1e9
-        kernels[k] = dict(ms=round(phase_ms[k], 5), algorithmic_bytes=tr[k], gbs=round(gbs, 1),
-                          tflops=round(fl[k] / (phase_ms[k] / 1e3) / 1e12, 3))
+        sec = phase_ms[k] / 1e3
+        kernels[k] = dict(ms=round(phase_ms[k], 5), algorithmic_bytes=int(tf[k]["bytes"]),
+                          gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3))
     kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
-    achieved = tr["radial"] / (phase_ms["radial"] / 1e3) / 1e9
-    roofline = dict(bound="hbm", kernel="radial propagator (k_radial_fp64)", achieved=round(achieved, 1),
-                    peak=hbm_peak, unit="GB/s", frac=round(achieved / hbm_peak, 4), traffic=None,
+    rad = kernels["radial"]
+    name = "k_radial_fp64" if precision == "fp64" else "k_radial_tc (tcgen05, 3xBF16)"
+    roofline = dict(bound="hbm", kernel=f"radial propagator ({name})", achieved=rad["gbs"], peak=hbm_peak,
+                    unit="GB/s", frac=round(rad["gbs"] / hbm_peak, 4), traffic=None,
                     peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom, kernels=kernels)
+    if tensor_peak:
+        roofline["tensor_frac_alg"] = round(rad["tflops"] / tensor_peak, 4)
+        roofline["tensor_frac_executed"] = round(3 * rad["tflops"] / tensor_peak, 4)
+        if roofline["tensor_frac_executed"] > roofline["frac"]:
+            roofline.update(bound="tensor", achieved=round(3 * rad["tflops"], 3), peak=tensor_peak,
+                            unit="TFLOP/s (executed split products)", frac=roofline["tensor_frac_executed"],
+                            peak_kind=f"{peak_kind} bf16_tflops")
+    # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU
+    fp64_inst = None
+    if args.compare_fp64 and (len(runs) > 1 or precision != "fp64"):
+        from ggbtddft_b200.engine import group_runs
+        total_s, units = 0.0, 0
+        for members in group_runs(runs):
+            one = TimePropagation([runs[members[0]]], precision="fp64", per_l=True, n_t=n_t)
+            one.step(args.warmup, h)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k = min(args.steps, 64)
+            a.record(stream)
+            one.step(k, h)
+            b.record(stream)
+            torch.cuda.synchronize()
+            per_step = a.elapsed_time(b) / 1e3 / k
+            one.close()
+            total_s += per_step * len(members)
+            units += sum(runs[i].n_orb for i in members)
+        rate = units / total_s
+        fp64_inst = dict(value=rate, unit="orbital-steps/s",
+                         how="each run of the workload stepped alone in the FP64 form (one time per grid, "
+                             "weighted by the runs on it), same GPU", speedup=round(value / rate, 2))
     return dict(value=value, ms=ms_max, units_per_step=units_per_step, desc=desc, precision=precision,
                 clocks=clk.summary(), roofline=roofline,
-                e2e=dict(value=e2e_value, unit="orbital-steps/s", h2d_bytes_per_step=int(h2d / args.steps),
-                         d2h_bytes_per_step=int(d2h / args.steps)),
-                gpu_launches=4 * args.steps * len(tp.groups))
+                e2e=None if e2e_value is None else dict(
+                    value=e2e_value, unit="orbital-steps/s", h2d_bytes_per_step=int(h2d / args.steps),
+                    d2h_bytes_per_step=int(d2h / args.steps)),
+                gpu_launches=4 * args.steps * len(tp.groups), fp64_per_instance=fp64_inst)
 
 
 def cpu_port_rate(runs, n_steps: int, warmup: int = 1):
@@ -272,6 +335,9 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")
+    ap.add_argument("--compare-fp64", type=int, default=1,
+                    help="also time the runs one at a time in the FP64 form (per-instance baseline)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -301,7 +367,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     res = run_ours(args, rank, world, dist)
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_sample_steps > 0:
         n_t = args.cpu_sample_steps + 4
         runs, _, _ = workload_runs(args.workload, n_t)
         rate, dt = cpu_port_rate(runs, args.cpu_sample_steps)
@@ -317,7 +383,7 @@ def main():
                     scaling="weak", vs_baseline=None, dtype="f64" if res["precision"] == "fp64" else "f32+split-bf16",
                     data="synthetic (seeded laser parameters; LDA ground state computed at set-up)", config=desc,
                     roofline=res["roofline"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
-                    gpu_launches=res["gpu_launches"])
+                    gpu_launches=res["gpu_launches"], fp64_per_instance=res["fp64_per_instance"])
         print(json.dumps(line))
     if dist:
         torch.distributed.destroy_process_group()

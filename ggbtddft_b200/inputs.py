@@ -20,6 +20,7 @@ library (``ggbtddft_b200/csrc``).
 from __future__ import annotations
 
 import dataclasses
+import functools
 import math
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -354,11 +355,12 @@ def coupling_matrix(coupling: str, n_l: int, m: int) -> np.ndarray:
     return u
 
 
+@functools.lru_cache(maxsize=32)
 def angular_eigensystems(n_l: int, n_m: int) -> Dict[str, Tuple[np.ndarray, np.ndarray]]:
     """V[m][l][j] and D[m][j] of each coupling, the workingData V%03d/D%03d files (internal.py:122-198).
 
     For each m the block l, j >= m of the coupling matrix is diagonalised with eigh; rows and
-    columns below m are zero.
+    columns below m are zero.  Cached per (n_l, n_m); the arrays are read-only.
     """
     out = {}
     for c in COUPLINGS:
@@ -369,6 +371,8 @@ def angular_eigensystems(n_l: int, n_m: int) -> Dict[str, Tuple[np.ndarray, np.n
             d, v = np.linalg.eigh(L[m:, m:])
             D[m, m:] = d
             V[m, m:, m:] = v
+        V.setflags(write=False)
+        D.setflags(write=False)
         out[c] = (V, D)
     return out
 
@@ -428,15 +432,21 @@ class Orbital:
     occ: int
 
 
-def bound_states(grid: RadialGrid, l: int, v: np.ndarray, count: int) -> Tuple[np.ndarray, np.ndarray]:
+def bound_states(grid: RadialGrid, l: int, v: np.ndarray, count: int,
+                 device: Optional[str] = None) -> Tuple[np.ndarray, np.ndarray]:
     """Lowest ``count`` eigen-pairs of the real radial Hamiltonian -T/2 + v + l(l+1)/2r^2.
 
     Eigenvectors are the DVR coefficients u_i (sum |u_i|^2 = 1), sign fixed so that the
-    largest-magnitude entry is positive.
+    largest-magnitude entry is positive.  ``device="cuda"`` diagonalises with torch in FP64.
     """
     H = -0.5 * grid.T + np.diag(v + l * (l + 1) / 2.0 / grid.r ** 2)
     H = 0.5 * (H + H.T)
-    e, u = np.linalg.eigh(H)
+    if device is not None:
+        import torch
+        e, u = torch.linalg.eigh(torch.from_numpy(H).to(device))
+        e, u = e.cpu().numpy(), u.cpu().numpy()
+    else:
+        e, u = np.linalg.eigh(H)
     e = e[:count]
     u = u[:, :count]
     for k in range(u.shape[1]):
@@ -497,7 +507,7 @@ class GroundState:
 
 def ground_state(grid: RadialGrid, Z: float, orbitals: Sequence[Orbital], interacting: bool,
                  correlation: bool = False, iterations: int = 200, mix: float = 0.3,
-                 tol: float = 1e-11) -> GroundState:
+                 tol: float = 1e-11, device: Optional[str] = None) -> GroundState:
     """Spherical Kohn-Sham LDA ground state on the grid (Slater exchange, optional PW92).
 
     The reference obtains its ground state from groundState.py (LDA + LB94 + Chachiyo), which is
@@ -514,7 +524,7 @@ def ground_state(grid: RadialGrid, Z: float, orbitals: Sequence[Orbital], intera
         en = np.zeros(len(orbitals))
         for l in ls:
             need = max(o.n - o.l for o in orbitals if o.l == l)
-            e, vecs = bound_states(grid, l, vtot, need)
+            e, vecs = bound_states(grid, l, vtot, need, device=device)
             for k, o in enumerate(orbitals):
                 if o.l == l:
                     u[k] = vecs[:, o.n - o.l - 1]

@@ -213,7 +213,7 @@ def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser
     gs = None if gs_cache is None else gs_cache.get(key)
     if gs is None:
         gs = I.ground_state(grid, spec.Z, spec.orbitals, interacting=spec.interacting,
-                            correlation=spec.correlation)
+                            correlation=spec.correlation, device=device)
         if gs_cache is not None:
             gs_cache[key] = gs
     full = I.steps_for_sin2(dt, laser.omega, laser.cycles)
@@ -242,3 +242,77 @@ def config_argon(n_steps=None, device=None) -> RunInputs:
     """Ar LDA: N_r=600, r_max=300, l_max=96, 800 nm, 1.4e14, 10 cycles, dt=0.02, mask 60 a.u."""
     return baseline_run("Ar", 600, 300.0, 96, 0.02, LaserSpec(1.4e14, 800.0, 10.0, 0.0), 60.0,
                         n_steps=n_steps, device=device)
+
+
+# ----------------------------------------------------------------------------------------------
+# ensembles (focal-volume scans)
+# ----------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class GridRung:
+    n_r: int
+    r_max: float
+    l_max: int
+
+
+# Grid ladders.  Runs are binned onto a few grids so that the runs of one grid share W (the radial
+# propagators depend on the atom, the grid, dt and the absorber, not on the laser).
+ARGON_LADDER = [GridRung(600, 300.0, 96), GridRung(700, 350.0, 112), GridRung(800, 400.0, 128),
+                GridRung(900, 450.0, 144), GridRung(1000, 500.0, 160)]
+HHE_LADDER = [GridRung(200, 100.0, 32), GridRung(400, 200.0, 64), GridRung(600, 300.0, 96),
+              GridRung(800, 400.0, 128)]
+
+
+def quiver_radius(laser: LaserSpec) -> float:
+    return laser.e0 / laser.omega ** 2
+
+
+def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = None, device=None,
+                   ladder: Sequence[GridRung] = ARGON_LADDER) -> List[RunInputs]:
+    """Argon LDA in-situ focal scan: I ~ U[0.8, 2]e14 W/cm^2, lambda ~ U[800, 1300] nm, 10-cycle sin^2,
+    dt = 0.02, 9 orbitals; each run goes on the ladder rung indexed by its wavelength
+    (longer wavelength -> larger excursion and higher cutoff -> larger grid and l_max)."""
+    rng = np.random.default_rng(seed)
+    I0 = rng.uniform(0.8e14, 2.0e14, n_runs)
+    lam = rng.uniform(800.0, 1300.0, n_runs)
+    return _ensemble("Ar", I0, lam, np.zeros(n_runs), 10.0, 0.02, n_steps, device, ladder,
+                     lambda l: min(len(ladder) - 1, int((l - 800.0) / 100.0)))
+
+
+def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None, device=None,
+                 ladder: Sequence[GridRung] = HHE_LADDER) -> List[RunInputs]:
+    """H/He-like scan: I log-uniform in [0.5, 3]e14, CEP ~ U[0, 2 pi), lambda ~ U[800, 1800] nm,
+    6-cycle sin^2, dt = 0.03; atoms alternate H / He; the rung is the smallest whose r_max covers
+    3 quiver radii plus the absorber."""
+    rng = np.random.default_rng(seed)
+    I0 = np.exp(rng.uniform(np.log(0.5e14), np.log(3.0e14), n_runs))
+    cep = rng.uniform(0.0, 2.0 * np.pi, n_runs)
+    lam = rng.uniform(800.0, 1800.0, n_runs)
+
+    def rung(i_run):
+        a = quiver_radius(LaserSpec(I0[i_run], lam[i_run], 6.0))
+        for k, g in enumerate(ladder):
+            if g.r_max * 0.8 >= 3.0 * a:
+                return k
+        return len(ladder) - 1
+    atoms = ["H" if i % 2 == 0 else "He" for i in range(n_runs)]
+    return _ensemble(atoms, I0, lam, cep, 6.0, 0.03, n_steps, device, ladder, None, rung_of_run=rung)
+
+
+def _ensemble(atom, I0, lam, cep, cycles, dt, n_steps, device, ladder, rung_of_lambda, rung_of_run=None):
+    n_runs = len(I0)
+    runs: List[RunInputs] = []
+    gs_cache: dict = {}
+    w_cache: dict = {}
+    for i in range(n_runs):
+        a = atom[i] if isinstance(atom, list) else atom
+        k = rung_of_run(i) if rung_of_run is not None else rung_of_lambda(lam[i])
+        g = ladder[k]
+        laser = LaserSpec(float(I0[i]), float(lam[i]), cycles, float(cep[i]))
+        key = (a, g.n_r, g.r_max, g.l_max)
+        run = baseline_run(a, g.n_r, g.r_max, g.l_max, dt, laser, 0.2 * g.r_max, n_steps=n_steps,
+                           device=device, gs_cache=gs_cache, W=w_cache.get(key))
+        w_cache[key] = run.W
+        run.name = f"{a}-{i}-N{g.n_r}-L{g.l_max}"
+        runs.append(run)
+    return runs

@@ -58,9 +58,15 @@ def test_fp64_odd_sizes_interacting(n_r, n_l):
 
 
 def test_fp64_hydrogen_config_shape():
-    """N_r = 200, l_max = 32, sin^2 pulse, cos^(1/8) mask: the hydrogen configuration's sizes."""
-    run = P.config_hydrogen(n_steps=60)
-    _compare_all(run)
+    """N_r = 200, l_max = 32, sin^2 pulse, cos^(1/8) mask: the hydrogen configuration's sizes.
+
+    The 60-step window is taken at the pulse centre: at the front of a sin^2 pulse E ~ 0 and the
+    dipole/acceleration of the ground state are rounding noise (~1e-10, dominated by the radial
+    product near r -> 0 under the r^-2 weight), which no two summation orders reproduce alike.
+    """
+    full = P.config_hydrogen()
+    mid = full.n_t // 2
+    _compare_all(full.with_field(full.E[mid:mid + 60]))
 
 
 def test_fp64_pw92_correlation():
