@@ -13,17 +13,17 @@ __device__ __forceinline__ double cf(const double* tab, int n_l, int l) {
   return (l >= 0 && l < n_l) ? tab[l] : 0.0;
 }
 
-template <class C>
+template <class C, int STRIDE = TR>
 __device__ __forceinline__ double xdot(const C* xs, int n_l, int a, int b, int lane) {
   if (a < 0 || a >= n_l || b < 0 || b >= n_l) return 0.0;
-  const C xa = xs[a * TR + lane];
-  const C xb = xs[b * TR + lane];
+  const C xa = xs[a * STRIDE + lane];
+  const C xb = xs[b * STRIDE + lane];
   return (double)xa.x * (double)xb.x + (double)xa.y * (double)xb.y;
 }
 
 // One multipole of one orbital's density at one radius, with the reference's literal l ranges
 // (hartreePotentialDensity.cuh:21-177, including the tail loop of L = 3 that restarts at N_l-4).
-template <class C>
+template <class C, int STRIDE = TR>
 __device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane,
                                     const double* coef, int n_m) {
   const double* cu = coef + ((size_t)CF_CU * n_m + m) * n_l;
@@ -36,37 +36,37 @@ __device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane
   double d = 0.0;
   if (L == 0) {
     for (int lp = m; lp < n_l; ++lp) {
-      const C v = xs[lp * TR + lane];
+      const C v = xs[lp * STRIDE + lane];
       d += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
     }
   } else if (L == 1) {
     int lp = m;
-    d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
+    d += cf(cu, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane);
     for (lp = m + 1; lp < n_l - 1; ++lp)
-      d += cf(cu, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+      d += cf(cu, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane) + cf(cd, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane);
     lp = n_l - 1;
-    d += cf(cd, n_l, lp) * xdot(xs, n_l, lp - 1, lp, lane);
+    d += cf(cd, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane);
   } else if (L == 2) {
     for (int lp = m; lp < m + 2; ++lp)
-      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+      d += cf(qu, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 2, lp, lane) + cf(pp, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp, lp, lane);
     for (int lp = m + 2; lp < n_l - 2; ++lp)
-      d += cf(qu, n_l, lp) * xdot(xs, n_l, lp + 2, lp, lane) + cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) +
-           cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+      d += cf(qu, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 2, lp, lane) + cf(qd, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp - 2, lp, lane) +
+           cf(pp, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp, lp, lane);
     for (int lp = n_l - 2; lp < n_l; ++lp)
-      d += cf(qd, n_l, lp) * xdot(xs, n_l, lp - 2, lp, lane) + cf(pp, n_l, lp) * xdot(xs, n_l, lp, lp, lane);
+      d += cf(qd, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp - 2, lp, lane) + cf(pp, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp, lp, lane);
   } else if (L == 3) {
     int lp = m;
-    d += cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+    d += cf(p3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 3, lp, lane);
     for (lp = m + 1; lp < m + 3; ++lp)
-      d += cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) + cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) +
-           cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+      d += cf(p3, n_l, lp - 1) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane) + cf(p3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane) +
+           cf(f3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 3, lp, lane);
     for (lp = m + 3; lp < n_l - 3; ++lp)
-      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
-           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot(xs, n_l, lp + 3, lp, lane);
+      d += cf(f3, n_l, lp - 3) * xdot<C, STRIDE>(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane) + cf(f3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 3, lp, lane);
     for (lp = n_l - 4; lp < n_l - 1; ++lp)
-      d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane) +
-           cf(p3, n_l, lp) * xdot(xs, n_l, lp + 1, lp, lane);
-    d += cf(f3, n_l, lp - 3) * xdot(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot(xs, n_l, lp - 1, lp, lane);
+      d += cf(f3, n_l, lp - 3) * xdot<C, STRIDE>(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane) +
+           cf(p3, n_l, lp) * xdot<C, STRIDE>(xs, n_l, lp + 1, lp, lane);
+    d += cf(f3, n_l, lp - 3) * xdot<C, STRIDE>(xs, n_l, lp - 3, lp, lane) + cf(p3, n_l, lp - 1) * xdot<C, STRIDE>(xs, n_l, lp - 1, lp, lane);
   }
   return d;
 }
@@ -89,18 +89,18 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Dipole and acceleration partial sums over this tile's radii for every l of one column
 // (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc).
-template <class C>
+template <class C, int STRIDE = TR>
 __device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m, int tile, int lane,
-                                 int warp, double rr, double fr2) {
+                                 int warp, int n_warps, double rr, double fr2) {
   const int n_l = g.n_l;
   const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
   const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
-  for (int l = warp; l < n_l; l += ANG_WARPS) {
+  for (int l = warp; l < n_l; l += n_warps) {
     double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
     if (l >= m) {
-      const double2 xl = to_d2(xs[l * TR + lane]);
-      const double2 xu = (l + 1 < n_l) ? to_d2(xs[(l + 1) * TR + lane]) : make_double2(0.0, 0.0);
-      const double2 xd = (l >= 1) ? to_d2(xs[(l - 1) * TR + lane]) : make_double2(0.0, 0.0);
+      const double2 xl = to_d2(xs[l * STRIDE + lane]);
+      const double2 xu = (l + 1 < n_l) ? to_d2(xs[(l + 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
+      const double2 xd = (l >= 1) ? to_d2(xs[(l - 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
       const double c_u = cu[l], c_d = cd[l];
       double2 z1, z2;
       if (l == m) {

@@ -87,7 +87,27 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
 #pragma unroll
       for (int q = 0; q < ANG_JB; ++q) acc[q] = make_double2(0.0, 0.0);
       const double* Sc = S + j0;
-      for (int l = m; l < n_l; ++l) {
+      int l = m;
+      // four l rows per iteration: 16 independent 16-byte loads of S in flight per thread
+      for (; l + 4 <= n_l; l += 4) {
+        double2 sv[4][ANG_JB / 2];
+        double2 xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          xv[u] = xs[(l + u) * TR + lane];
+          const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)(l + u) * g.ldS);
+#pragma unroll
+          for (int h = 0; h < ANG_JB / 2; ++h) sv[u][h] = __ldg(Srow + h);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int h = 0; h < ANG_JB / 2; ++h) {
+            acc[2 * h].x += sv[u][h].x * xv[u].x;     acc[2 * h].y += sv[u][h].x * xv[u].y;
+            acc[2 * h + 1].x += sv[u][h].y * xv[u].x; acc[2 * h + 1].y += sv[u][h].y * xv[u].y;
+          }
+      }
+      for (; l < n_l; ++l) {
         const double2 xv = xs[l * TR + lane];
         const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)l * g.ldS);
 #pragma unroll
@@ -126,7 +146,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile(g, xs, col, m, tile, lane, warp, rr, fr2);
+    observables_tile(g, xs, col, m, tile, lane, warp, ANG_WARPS, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
     for (int L = warp; L < n_den; L += ANG_WARPS) {
       const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
@@ -172,7 +192,22 @@ k_radial_fp64(int n_r, int n_cols, const double2* __restrict__ W, const double2*
     }
     __syncthreads();
     const int kmax = min(RAD_KC, n_r - k0);
-    for (int kk = 0; kk < kmax; ++kk) {
+    int kk = 0;
+    // eight W loads in flight per thread before the FMAs that consume them
+    for (; kk + 8 <= kmax; kk += 8) {
+      double2 w[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) w[u] = iv ? __ldcs(Wl + (size_t)(k0 + kk + u) * n_r + i) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int c = 0; c < TC; ++c) {
+          const double2 x = xsm[c][kk + u];
+          acc[c].x += w[u].x * x.x - w[u].y * x.y;
+          acc[c].y += w[u].x * x.y + w[u].y * x.x;
+        }
+    }
+    for (; kk < kmax; ++kk) {
       const double2 w = iv ? __ldcs(Wl + (size_t)(k0 + kk) * n_r + i) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int c = 0; c < TC; ++c) {

@@ -1,14 +1,19 @@
 // Split-precision form of the step.
 //
-//  k_split_w        one-time: W[l][k][i] (complex128) -> A(i,k) = W[l][k][i] as four BF16 planes
-//                   (Wr hi, Wr lo, Wi hi, Wi lo), K-major, zero padded, for TMA.
+//  k_split_w        one-time: W[l][k][i] (complex128) -> A(i,k) = W[l][k][i] as six BF16 planes
+//                   (Wr hi, mid, lo, Wi hi, mid, lo: three terms, residual 2^-25 of |W|), K-major,
+//                   zero padded, for TMA.  Three terms, because W is applied every step: a 2^-17
+//                   representation error of a constant unitary operator is a fixed non-unitarity that
+//                   compounds over tens of thousands of steps, while the rounding of the (changing)
+//                   orbitals only random-walks.
 //  k_angular_f32    the angular half-step chain of k_angular_fp64 in FP32 on complex64 orbitals;
 //                   the first half writes the radial B operand directly as BF16 hi/lo planes, the
 //                   second half keeps the FP64 density/dipole partial sums of the FP64 form.
 //  k_radial_tc      x_l <- A_l x_l on tcgen05: TMA-staged tiles (128 radii x 32 k per plane),
-//                   3xBF16 split products (hi*hi + hi*lo + lo*hi) for each of the four real
-//                   products of the complex GEMM, the -Wi Xi term through the A-negate bit of the
-//                   instruction descriptor, FP32 accumulators Re/Im in tensor memory.
+//                   split products W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (only W_l x_l,
+//                   ~2^-24, dropped) for each of the four real products of the complex GEMM, the
+//                   -Wi Xi term through the A-negate bit of the instruction descriptor, FP32
+//                   accumulators Re/Im in tensor memory.
 //  The potentials/observables kernel (k_finalize) is shared with the FP64 form.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -20,6 +25,7 @@
 #include "../../include/ggbtddft.h"
 #include "ggb_angular.cuh"
 #include "ggb_mixed.cuh"
+#include "ggb_tc_common.cuh"
 
 namespace ggb {
 
@@ -31,10 +37,19 @@ __device__ __forceinline__ void split_bf16(double v, __nv_bfloat16& hi, __nv_bfl
   hi = __double2bfloat16(v);
   lo = __double2bfloat16(v - (double)__bfloat162float(hi));
 }
+__device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16& hi, __nv_bfloat16& mid, __nv_bfloat16& lo) {
+  hi = __double2bfloat16(v);
+  const double r1 = v - (double)__bfloat162float(hi);
+  mid = __double2bfloat16(r1);
+  lo = __double2bfloat16(r1 - (double)__bfloat162float(mid));
+}
 __device__ __forceinline__ void split_bf16f(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
   hi = __float2bfloat16_rn(v);
   lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
+
+constexpr int W_PLANES = 6;   // Wr hi, mid, lo, Wi hi, mid, lo
+constexpr int S_PLANES = 3;   // S^T hi, mid, lo
 
 // 32x32 tiles through shared memory: read W[l][k][i] along i, write A(i,k) along k.
 __global__ void k_split_w(const double2* __restrict__ W, __nv_bfloat16* __restrict__ Wsp, int n_r, int rows_pad,
@@ -49,20 +64,42 @@ __global__ void k_split_w(const double2* __restrict__ W, __nv_bfloat16* __restri
   }
   __syncthreads();
   const size_t plane = (size_t)rows_pad * k_pad;
-  __nv_bfloat16* base = Wsp + (size_t)l * 4 * plane;
+  __nv_bfloat16* base = Wsp + (size_t)l * W_PLANES * plane;
   for (int q = ty; q < 32; q += 8) {
     const int i = i0 + q, k = k0 + tx;
     if (i < rows_pad && k < k_pad) {
       const double2 w = t[tx][q];
-      __nv_bfloat16 rh, rl, ih, il;
-      split_bf16(w.x, rh, rl);
-      split_bf16(w.y, ih, il);
+      __nv_bfloat16 rh, rm, rl, ih, im, il;
+      split3_bf16(w.x, rh, rm, rl);
+      split3_bf16(w.y, ih, im, il);
       const size_t o = (size_t)i * k_pad + k;
       base[o] = rh;
-      base[plane + o] = rl;
-      base[2 * plane + o] = ih;
-      base[3 * plane + o] = il;
+      base[plane + o] = rm;
+      base[2 * plane + o] = rl;
+      base[3 * plane + o] = ih;
+      base[4 * plane + o] = im;
+      base[5 * plane + o] = il;
     }
+  }
+}
+
+// S^T planes for the tensor-core angular chain: St[mat][m][plane][j][l] = 3-term split of S[mat][m][l][j],
+// zero for j >= N_l or l >= N_l.
+__global__ void k_build_st(const double* __restrict__ mats, __nv_bfloat16* __restrict__ St, int n_mats, int n_m,
+                           int n_l, int ldS, int rows, int lk) {
+  const size_t total = (size_t)n_mats * n_m * rows * lk;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int l = (int)(i % lk);
+    const int j = (int)((i / lk) % rows);
+    const size_t mm = i / ((size_t)lk * rows);      // mat * n_m + m
+    double v = 0.0;
+    if (j < n_l && l < n_l) v = mats[(mm * n_l + l) * ldS + j];
+    __nv_bfloat16 hi, mid, lo;
+    split3_bf16(v, hi, mid, lo);
+    const size_t plane = (size_t)rows * lk;
+    St[mm * S_PLANES * plane + (size_t)j * lk + l] = hi;
+    St[mm * S_PLANES * plane + plane + (size_t)j * lk + l] = mid;
+    St[mm * S_PLANES * plane + 2 * plane + (size_t)j * lk + l] = lo;
   }
 }
 
@@ -198,13 +235,13 @@ k_angular_f32(GroupArgs g, MixArgs mx, int half, const float2* __restrict__ xin,
         b[3 * plane] = il;
       }
     }
-  } else if (rv) {
+  } else if (rv && xout) {
     for (int l = warp; l < n_l; l += ANG_WARPS) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * TR + lane];
   }
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile(g, xs, col, m, tile, lane, warp, rr, fr2);
+    observables_tile(g, xs, col, m, tile, lane, warp, ANG_WARPS, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;
     for (int L = warp; L < n_den; L += ANG_WARPS) {
       const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
@@ -222,88 +259,59 @@ static size_t angular_smem_f32(int n_l) { return 2 * (size_t)n_l * TR * sizeof(f
 constexpr int RT_BM = 128;         // radii per tile (MMA M)
 constexpr int RT_BK = 32;          // k per stage (64 bytes of BF16 per row: 64-byte swizzle)
 constexpr int RT_THREADS = 192;    // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
-constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // bounded waits give up after 2 s
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ uint64_t gtimer() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t n) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Wait for the phase of `parity`; gives up (returns false, raises the abort flag) after the limit
-// or as soon as another role has aborted.
-__device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
-  const uint64_t t0 = gtimer();
-  while (!mbar_try(b, parity)) {
-    if (*abort_flag) return false;
-    if (gtimer() - t0 > WAIT_LIMIT_NS) {
-      *abort_flag = 1;
-      return false;
-    }
-  }
-  return true;
-}
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
-      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
-        "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_commit(uint64_t* b) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b))
-               : "memory");
-}
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
-}
-// Shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 bytes, 8-row groups 512 B apart.
-__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
-  d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: next 8-row group
-  d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
-  d |= (uint64_t)4 << 61;                           // layout: 64-byte swizzle
-  return d;
-}
-// Instruction descriptor, kind::f16: BF16 x BF16 -> FP32, both K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_bf16(int n, bool negate_a) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((negate_a ? 1u : 0u) << 13) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(RT_BM >> 4) << 24);
-}
+// Instruction descriptor of the radial product: M = 128 radii, N = n columns.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, bool negate_a) { return idesc_bf16_mn(RT_BM, n, negate_a); }
+// Shared-memory descriptor of the radial tiles: K-major, 64-byte swizzle, 64-byte rows.
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) { return sdesc_kmajor(saddr, 64, 4); }
 
 template <int BN>
 struct RadialTile {
   static constexpr int A_PLANE = RT_BM * RT_BK * 2;       // bytes of one plane tile of W
   static constexpr int B_PLANE = BN * RT_BK * 2;          // bytes of one plane tile of x
-  static constexpr int STAGE = 4 * A_PLANE + 4 * B_PLANE;
+  static constexpr int A_STAGE = W_PLANES * A_PLANE;
+  static constexpr int STAGE = A_STAGE + 4 * B_PLANE;
   static constexpr int TMEM_COLS = (2 * BN <= 32) ? 32 : (2 * BN <= 64) ? 64 : (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
 };
+
+// The MMAs of one 32-wide k block of the radial product into D_re / D_im:
+//   Re += Wr Xr - Wi Xi,  Im += Wr Xi + Wi Xr,  each real product W X as
+//   W_h X_h + W_h X_l + W_m X_h + W_m X_l + W_l X_h  (W in three BF16 terms, X in two).
+template <int BN>
+__device__ __forceinline__ void radial_mma_kblock(uint32_t sa, uint32_t sb, uint32_t d_re, uint32_t d_im,
+                                                  bool first, uint32_t a_plane, uint32_t b_plane) {
+  const uint32_t id_pos = idesc_bf16(BN, false), id_neg = idesc_bf16(BN, true);
+#pragma unroll
+  for (int kk = 0; kk < RT_BK / 16; ++kk) {
+    const uint32_t ko = kk * 32;  // 16 BF16 = 32 bytes along k
+    uint64_t w[W_PLANES], x[4];
+#pragma unroll
+    for (int p = 0; p < W_PLANES; ++p) w[p] = sdesc_sw64(sa + p * a_plane + ko);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) x[p] = sdesc_sw64(sb + p * b_plane + ko);
+    const uint32_t acc0 = (!first || kk > 0) ? 1u : 0u;
+    // w: 0-2 Wr (h, m, l), 3-5 Wi (h, m, l);  x: 0 Xr h, 1 Xr l, 2 Xi h, 3 Xi l
+    tc_mma(d_re, w[0], x[0], id_pos, acc0);
+    tc_mma(d_re, w[0], x[1], id_pos, 1u);
+    tc_mma(d_re, w[1], x[0], id_pos, 1u);
+    tc_mma(d_re, w[1], x[1], id_pos, 1u);
+    tc_mma(d_re, w[2], x[0], id_pos, 1u);
+    tc_mma(d_re, w[3], x[2], id_neg, 1u);
+    tc_mma(d_re, w[3], x[3], id_neg, 1u);
+    tc_mma(d_re, w[4], x[2], id_neg, 1u);
+    tc_mma(d_re, w[4], x[3], id_neg, 1u);
+    tc_mma(d_re, w[5], x[2], id_neg, 1u);
+    tc_mma(d_im, w[0], x[2], id_pos, acc0);
+    tc_mma(d_im, w[0], x[3], id_pos, 1u);
+    tc_mma(d_im, w[1], x[2], id_pos, 1u);
+    tc_mma(d_im, w[1], x[3], id_pos, 1u);
+    tc_mma(d_im, w[2], x[2], id_pos, 1u);
+    tc_mma(d_im, w[3], x[0], id_pos, 1u);
+    tc_mma(d_im, w[3], x[1], id_pos, 1u);
+    tc_mma(d_im, w[4], x[0], id_pos, 1u);
+    tc_mma(d_im, w[4], x[1], id_pos, 1u);
+    tc_mma(d_im, w[5], x[0], id_pos, 1u);
+  }
+}
 
 template <int BN>
 __global__ void __launch_bounds__(RT_THREADS, 1)
@@ -350,7 +358,7 @@ k_radial_tc(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
         uint8_t* st = smem + (size_t)s * T::STAGE;
         mbar_expect_tx(&full_bar[s], T::STAGE);
         tma_load_4d(st, &tmW, kb * RT_BK, m0, 0, l, &full_bar[s]);
-        tma_load_4d(st + 4 * T::A_PLANE, &tmX, kb * RT_BK, c0, 0, l, &full_bar[s]);
+        tma_load_4d(st + T::A_STAGE, &tmX, kb * RT_BK, c0, 0, l, &full_bar[s]);
         issued = kb + 1;
       }
       // never leave copies in flight: on abort, wait (bounded) for every issued stage to land
@@ -364,7 +372,6 @@ k_radial_tc(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t id_pos = idesc_bf16(BN, false), id_neg = idesc_bf16(BN, true);
       const uint32_t d_re = tmem, d_im = tmem + BN;
       int done = 0;
       for (int kb = 0; kb < n_k_blocks; ++kb) {
@@ -372,30 +379,7 @@ k_radial_tc(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
         if (!mbar_wait(&full_bar[s], (kb / stages) & 1, abort_p)) break;
         tc_fence_after();
         const uint32_t sa = smem_u32(smem + (size_t)s * T::STAGE);
-        const uint32_t sb = sa + 4 * T::A_PLANE;
-#pragma unroll
-        for (int kk = 0; kk < RT_BK / 16; ++kk) {
-          const uint32_t ko = kk * 32;  // 16 BF16 = 32 bytes along k
-          const uint64_t wrh = sdesc_sw64(sa + 0 * T::A_PLANE + ko), wrl = sdesc_sw64(sa + 1 * T::A_PLANE + ko);
-          const uint64_t wih = sdesc_sw64(sa + 2 * T::A_PLANE + ko), wil = sdesc_sw64(sa + 3 * T::A_PLANE + ko);
-          const uint64_t xrh = sdesc_sw64(sb + 0 * T::B_PLANE + ko), xrl = sdesc_sw64(sb + 1 * T::B_PLANE + ko);
-          const uint64_t xih = sdesc_sw64(sb + 2 * T::B_PLANE + ko), xil = sdesc_sw64(sb + 3 * T::B_PLANE + ko);
-          const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-          // Re: Wr Xr - Wi Xi
-          tc_mma(d_re, wrh, xrh, id_pos, acc0);
-          tc_mma(d_re, wrh, xrl, id_pos, 1u);
-          tc_mma(d_re, wrl, xrh, id_pos, 1u);
-          tc_mma(d_re, wih, xih, id_neg, 1u);
-          tc_mma(d_re, wih, xil, id_neg, 1u);
-          tc_mma(d_re, wil, xih, id_neg, 1u);
-          // Im: Wr Xi + Wi Xr
-          tc_mma(d_im, wrh, xih, id_pos, acc0);
-          tc_mma(d_im, wrh, xil, id_pos, 1u);
-          tc_mma(d_im, wrl, xih, id_pos, 1u);
-          tc_mma(d_im, wih, xrh, id_pos, 1u);
-          tc_mma(d_im, wih, xrl, id_pos, 1u);
-          tc_mma(d_im, wil, xrh, id_pos, 1u);
-        }
+        radial_mma_kblock<BN>(sa, sa + T::A_STAGE, d_re, d_im, kb == 0, T::A_PLANE, T::B_PLANE);
         tc_commit(&empty_bar[s]);   // frees the stage once these MMAs have read it
         done = kb + 1;
       }
@@ -454,6 +438,136 @@ k_radial_tc(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
   }
 }
 
+// Persistent form: one CTA per SM walks the (M tile, N tile, l) tiles with stride gridDim.x.  The
+// stage ring (TMA -> MMA) runs across tile boundaries without draining, and the accumulators are
+// double-buffered in tensor memory so the epilogue of one tile overlaps the MMAs of the next.
+template <int BN>
+__global__ void __launch_bounds__(RT_THREADS, 1)
+k_radial_tc_persistent(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmX, int n_r,
+                       int n_cols, int n_l, int n_k_blocks, int stages, float2* __restrict__ Y, unsigned* status) {
+  using T = RadialTile<BN>;
+  constexpr int TMEM_COLS = 2 * T::TMEM_COLS;   // two accumulator buffers
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ uint64_t full_bar[8], empty_bar[8], accf_bar[2], acce_bar[2], drain_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m_tiles = (n_r + RT_BM - 1) / RT_BM, n_tiles = (n_cols + BN - 1) / BN;
+  const int total = m_tiles * n_tiles * n_l;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf_bar[b], 1);
+      mbar_init(&acce_bar[b], 4);   // the four epilogue warps release a buffer
+    }
+    mbar_init(&drain_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(&tmem_slot, TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  volatile int* abort_p = &abort_flag;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+        const int mt = tile % m_tiles, rest = tile / m_tiles, nt = rest % n_tiles, l = rest / n_tiles;
+        for (int kb = 0; kb < n_k_blocks; ++kb, ++it) {
+          const int s = it % stages;
+          if (it >= stages && !mbar_wait(&empty_bar[s], ((it / stages) & 1) ^ 1, abort_p)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + (size_t)s * T::STAGE;
+          mbar_expect_tx(&full_bar[s], T::STAGE);
+          tma_load_4d(st, &tmW, kb * RT_BK, mt * RT_BM, 0, l, &full_bar[s]);
+          tma_load_4d(st + T::A_STAGE, &tmX, kb * RT_BK, nt * BN, 0, l, &full_bar[s]);
+        }
+      }
+      if (!ok)
+        for (int q = (it > stages ? it - stages : 0); q < it; ++q) mbar_drain(&full_bar[q % stages], (q / stages) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int it = 0, local = 0;
+      for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++local) {
+        const int buf = local & 1;
+        // the epilogue must have drained this buffer (its use two tiles back)
+        if (local >= 2 && !mbar_wait(&acce_bar[buf], ((local >> 1) - 1) & 1, abort_p)) break;
+        tc_fence_after();
+        const uint32_t d_re = tmem + buf * T::TMEM_COLS, d_im = d_re + BN;
+        bool ok = true;
+        for (int kb = 0; kb < n_k_blocks; ++kb, ++it) {
+          const int s = it % stages;
+          if (!mbar_wait(&full_bar[s], (it / stages) & 1, abort_p)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + (size_t)s * T::STAGE);
+          radial_mma_kblock<BN>(sa, sa + T::A_STAGE, d_re, d_im, kb == 0, T::A_PLANE, T::B_PLANE);
+          tc_commit(&empty_bar[s]);
+        }
+        tc_commit(&accf_bar[buf]);
+        if (!ok) break;
+      }
+    }
+  } else {
+    const int q = warp & 3;
+    const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+    int local = 0;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++local) {
+      const int buf = local & 1;
+      const int mt = tile % m_tiles, rest = tile / m_tiles, nt = rest % n_tiles, l = rest / n_tiles;
+      const bool ok = mbar_wait(&accf_bar[buf], (local >> 1) & 1, abort_p);
+      tc_fence_after();
+      if (!ok) break;
+      const int i = mt * RT_BM + 32 * q + lane, c0 = nt * BN;
+      const uint32_t d_re = tmem + buf * T::TMEM_COLS, d_im = d_re + BN;
+#pragma unroll 1
+      for (int cc = 0; cc < BN; cc += 16) {
+        uint32_t re[16], im[16];
+        tmem_ld16(d_re + lane_base + cc, re);
+        tmem_ld16(d_im + lane_base + cc, im);
+        tmem_ld_wait();
+        if (i < n_r) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + cc + j;
+            if (c < n_cols)
+              Y[((size_t)l * n_cols + c) * n_r + i] = make_float2(__uint_as_float(re[j]), __uint_as_float(im[j]));
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce_bar[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicOr(status, ST_TC_TIMEOUT);
+  if (warp == 1) {
+    if (abort_flag && lane == 0) {
+      // the drain barrier completes once every MMA this thread issued is done
+      tc_commit(&drain_bar);
+      mbar_drain(&drain_bar, 0);
+    }
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
 template <int BN>
 static size_t radial_smem(int stages) {
   return (size_t)stages * RadialTile<BN>::STAGE + 1024;
@@ -479,13 +593,14 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 4-D BF16 tensor (k, rows, plane, l) with a (32, box_rows, 4, 1) box and 64-byte swizzle.
-static bool make_map(CUtensorMap* map, void* base, int k_pad, int rows, int n_l, int box_rows) {
+// 4-D BF16 tensor (k, rows, plane, l) with a (32, box_rows, planes, 1) box and 64-byte swizzle.
+static bool make_map(CUtensorMap* map, void* base, int k_pad, int rows, int planes, int n_l, int box_rows) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return false;
-  cuuint64_t dims[4] = {(cuuint64_t)k_pad, (cuuint64_t)rows, 4, (cuuint64_t)n_l};
-  cuuint64_t strides[3] = {(cuuint64_t)k_pad * 2, (cuuint64_t)rows * k_pad * 2, (cuuint64_t)4 * rows * k_pad * 2};
-  cuuint32_t box[4] = {RT_BK, (cuuint32_t)box_rows, 4, 1};
+  cuuint64_t dims[4] = {(cuuint64_t)k_pad, (cuuint64_t)rows, (cuuint64_t)planes, (cuuint64_t)n_l};
+  cuuint64_t strides[3] = {(cuuint64_t)k_pad * 2, (cuuint64_t)rows * k_pad * 2,
+                           (cuuint64_t)planes * rows * k_pad * 2};
+  cuuint32_t box[4] = {RT_BK, (cuuint32_t)box_rows, (cuuint32_t)planes, 1};
   cuuint32_t es[4] = {1, 1, 1, 1};
   return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -510,11 +625,15 @@ static int pick_bn(int n_cols) {
 
 template <int BN>
 static cudaError_t configure_radial(int stages) {
-  return cudaFuncSetAttribute(k_radial_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)radial_smem<BN>(stages));
+  cudaError_t e = cudaFuncSetAttribute(k_radial_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)radial_smem<BN>(stages));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_radial_tc_persistent<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)radial_smem<BN>(stages));
 }
 
 static int stages_for(int bn) {
-  const int stage = 4 * RT_BM * RT_BK * 2 + 4 * bn * RT_BK * 2;
+  const int stage = W_PLANES * RT_BM * RT_BK * 2 + 4 * bn * RT_BK * 2;
   int s = (200 * 1024) / stage;
   if (s > 8) s = 8;
   if (s < 2) s = 2;
@@ -540,7 +659,7 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
   const size_t nxs = (size_t)n_l * 4 * m.cols_pad * m.k_pad;
   MX_CK(cudaMalloc(&m.Xsp, nxs * sizeof(__nv_bfloat16)));
   MX_CK(cudaMemset(m.Xsp, 0, nxs * sizeof(__nv_bfloat16)));
-  const size_t nws = (size_t)n_l * 4 * m.rows_pad * m.k_pad;
+  const size_t nws = (size_t)n_l * W_PLANES * m.rows_pad * m.k_pad;
   MX_CK(cudaMalloc(&m.Wsp, nws * sizeof(__nv_bfloat16)));
   const dim3 tb(32, 8), tg((m.rows_pad + 31) / 32, (m.k_pad + 31) / 32, n_l);
   k_split_w<<<tg, tb>>>(W_fp64, m.Wsp, n_r, m.rows_pad, m.k_pad);
@@ -553,9 +672,32 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
   MX_CK(cudaMalloc(&m.mats_f, n_mat_el * sizeof(float)));
   k_d2f_real<<<256, 256>>>(a.mats, m.mats_f, n_mat_el);
   MX_CK(cudaGetLastError());
-  if (!make_map(&m.tmW, m.Wsp, m.k_pad, m.rows_pad, n_l, RT_BM) || !make_map(&m.tmX, m.Xsp, m.k_pad, m.cols_pad, n_l, m.bn)) {
+  if (!make_map(&m.tmW, m.Wsp, m.k_pad, m.rows_pad, W_PLANES, n_l, RT_BM) ||
+      !make_map(&m.tmX, m.Xsp, m.k_pad, m.cols_pad, 4, n_l, m.bn)) {
     err = "cuTensorMapEncodeTiled failed";
     return GGB_ERR_CUDA;
+  }
+  // tensor-core angular chain (falls back to the FP32 chain when N_l does not fit its tiles)
+  if (angular_tc_config(n_l, m.at_k_atoms, m.at_m_tiles, m.at_stages, m.at_smem) == 0) {
+    const int rows = 128 * m.at_m_tiles, lk = 64 * m.at_k_atoms;
+    const size_t nst = (size_t)n_mats * a.n_m * S_PLANES * rows * lk;
+    MX_CK(cudaMalloc(&m.St, nst * sizeof(__nv_bfloat16)));
+    k_build_st<<<512, 256>>>(a.mats, m.St, n_mats, a.n_m, n_l, a.ldS, rows, lk);
+    MX_CK(cudaGetLastError());
+    EncodeTiledFn enc = encode_fn();
+    cuuint64_t dims[5] = {(cuuint64_t)lk, (cuuint64_t)rows, S_PLANES, (cuuint64_t)a.n_m, (cuuint64_t)n_mats};
+    cuuint64_t strides[4] = {(cuuint64_t)lk * 2, (cuuint64_t)rows * lk * 2, (cuuint64_t)S_PLANES * rows * lk * 2,
+                             (cuuint64_t)a.n_m * S_PLANES * rows * lk * 2};
+    cuuint32_t box[5] = {64, 128, 1, 1, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    if (!enc || enc(&m.tmS, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, m.St, dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      err = "cuTensorMapEncodeTiled (angular S^T) failed";
+      return GGB_ERR_CUDA;
+    }
+    MX_CK(angular_tc_configure());
+    m.angular_tc = true;
   }
   int dev = 0, optin = 0;
   MX_CK(cudaGetDevice(&dev));
@@ -572,6 +714,7 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
     case 64: MX_CK(configure_radial<64>(m.stages)); m.smem = radial_smem<64>(m.stages); break;
     default: MX_CK(configure_radial<128>(m.stages)); m.smem = radial_smem<128>(m.stages); break;
   }
+  MX_CK(cudaDeviceGetAttribute(&m.persistent_ctas, cudaDevAttrMultiProcessorCount, dev));
   MX_CK(cudaDeviceSynchronize());
   m.ready = true;
   return GGB_OK;
@@ -592,8 +735,19 @@ int mixed_store_orbitals(MixedGroup& m, const GroupArgs& a, double2* x_fp64) {
 }
 
 static void launch_radial_tc(MixedGroup& m, const GroupArgs& a, cudaStream_t s) {
-  const dim3 grid((a.n_r + RT_BM - 1) / RT_BM, (a.n_cols + m.bn - 1) / m.bn, a.n_l);
   const int nkb = m.k_pad / RT_BK;
+  if (m.persistent_ctas > 0) {
+    const int tiles = ((a.n_r + RT_BM - 1) / RT_BM) * ((a.n_cols + m.bn - 1) / m.bn) * a.n_l;
+    const dim3 g(tiles < m.persistent_ctas ? tiles : m.persistent_ctas);
+    switch (m.bn) {
+      case 16: k_radial_tc_persistent<16><<<g, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, a.n_l, nkb, m.stages, m.Y, a.status); break;
+      case 32: k_radial_tc_persistent<32><<<g, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, a.n_l, nkb, m.stages, m.Y, a.status); break;
+      case 64: k_radial_tc_persistent<64><<<g, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, a.n_l, nkb, m.stages, m.Y, a.status); break;
+      default: k_radial_tc_persistent<128><<<g, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, a.n_l, nkb, m.stages, m.Y, a.status); break;
+    }
+    return;
+  }
+  const dim3 grid((a.n_r + RT_BM - 1) / RT_BM, (a.n_cols + m.bn - 1) / m.bn, a.n_l);
   switch (m.bn) {
     case 16: k_radial_tc<16><<<grid, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, nkb, m.stages, m.Y, a.status); break;
     case 32: k_radial_tc<32><<<grid, RT_THREADS, m.smem, s>>>(m.tmW, m.tmX, a.n_r, a.n_cols, nkb, m.stages, m.Y, a.status); break;
@@ -615,16 +769,31 @@ void mixed_init(MixedGroup& m, const GroupArgs& a, const double2*, cudaStream_t 
   launch_angular_mixed(m, a, 2, m.X, m.X, false, 1, s);
 }
 
+static void angular_half(MixedGroup& m, const GroupArgs& a, int half, cudaStream_t s) {
+  if (m.angular_tc) {
+    if (half == 0) {
+      launch_angular_tc(m, a, 0, m.X, nullptr, s);
+    } else {
+      launch_angular_tc(m, a, 1, m.Y, m.X, s);
+      // FP64 density and dipole partial sums of the new orbitals (empty chain, no write-back)
+      launch_angular_mixed(m, a, 2, m.X, nullptr, false, 1, s);
+    }
+  } else {
+    if (half == 0) launch_angular_mixed(m, a, 0, m.X, nullptr, true, 0, s);
+    else launch_angular_mixed(m, a, 1, m.Y, m.X, false, 1, s);
+  }
+}
+
 void mixed_step(MixedGroup& m, const GroupArgs& a, cudaStream_t s) {
-  launch_angular_mixed(m, a, 0, m.X, nullptr, true, 0, s);
+  angular_half(m, a, 0, s);
   launch_radial_tc(m, a, s);
-  launch_angular_mixed(m, a, 1, m.Y, m.X, false, 1, s);
+  angular_half(m, a, 1, s);
 }
 
 void mixed_phase(MixedGroup& m, const GroupArgs& a, int phase, cudaStream_t s) {
-  if (phase == 0) launch_angular_mixed(m, a, 0, m.X, nullptr, true, 0, s);
+  if (phase == 0) angular_half(m, a, 0, s);
   if (phase == 1) launch_radial_tc(m, a, s);
-  if (phase == 2) launch_angular_mixed(m, a, 1, m.Y, m.X, false, 1, s);
+  if (phase == 2) angular_half(m, a, 1, s);
 }
 
 void mixed_release(MixedGroup& m) {
@@ -633,6 +802,7 @@ void mixed_release(MixedGroup& m) {
   cudaFree(m.Xsp);
   cudaFree(m.Wsp);
   cudaFree(m.mats_f);
+  cudaFree(m.St);
   m = MixedGroup();
 }
 

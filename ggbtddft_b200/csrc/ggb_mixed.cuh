@@ -23,6 +23,7 @@ struct MixedGroup {
   int cols_pad = 0;     // n_cols rounded up to the N tile (zero columns keep every TMA box in bounds)
   int stages = 4;
   size_t smem = 0;
+  int persistent_ctas = 0;  // > 0: persistent radial launch with this many CTAs (one per SM)
   float2* X = nullptr;              // state [N_l][n_cols][N_r]
   float2* Y = nullptr;              // radial output [N_l][n_cols][N_r]
   __nv_bfloat16* Xsp = nullptr;     // radial B operand [N_l][4][cols_pad][k_pad]  (re hi, re lo, im hi, im lo)
@@ -30,7 +31,18 @@ struct MixedGroup {
   float* mats_f = nullptr;          // chain matrices in FP32
   CUtensorMap tmW;
   CUtensorMap tmX;
+  // tensor-core angular chain
+  bool angular_tc = false;
+  __nv_bfloat16* St = nullptr;      // S^T planes [mat][m][hi,lo][m_tiles*128 (j)][k_atoms*64 (l)]
+  CUtensorMap tmS;
+  int at_k_atoms = 0, at_m_tiles = 0, at_stages = 0;
+  size_t at_smem = 0;
 };
+
+int angular_tc_config(int n_l, int& k_atoms, int& m_tiles, int& stages, size_t& smem);
+cudaError_t angular_tc_configure();
+void launch_angular_tc(const MixedGroup& mg, const GroupArgs& a, int half, const float2* xin, float2* xout,
+                       cudaStream_t s);
 
 int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precision, std::string& err);
 int mixed_load_orbitals(MixedGroup& m, const GroupArgs& a, const double2* x_fp64);
