@@ -51,7 +51,8 @@ _lib = None
 
 EXPORTS = ("ggb_create", "ggb_set_grid", "ggb_set_radial_propagators", "ggb_set_angular", "ggb_set_orbitals",
            "ggb_set_field", "ggb_step", "ggb_get_step", "ggb_get_observables", "ggb_get_orbitals",
-           "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase")
+           "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase",
+           "ggb_observables_noalloc")
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -81,6 +82,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_status": ([P, ctypes.c_char_p, I_], I_),
         "ggb_destroy": ([P], None),
         "ggb_version": ([], ctypes.c_char_p),
+        "ggb_observables_noalloc": ([P, P, P, I_, I_, I_, P, P, P, P], I_),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

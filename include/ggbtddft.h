@@ -143,6 +143,25 @@ int ggb_status(ggb_ctx* ctx, char* msg, int len);
 /* Release every device buffer of the context. */
 void ggb_destroy(ggb_ctx* ctx);
 
+/* Observables of a set of orbitals without any device allocation.  No counterpart in the
+   reference.  For callers that cannot call cudaMalloc: code running inside another framework's
+   memory pool, which must own every device allocation, or a process that reserved all device
+   memory up front.
+   From orbitals x[l][kso][r] (complex128), the grid r[N_r] and the azimuthal numbers m[N_kso]
+   (int32) it writes dip[l][kso] and acc[l][kso] (complex128: the per-(l, orbital) sums that
+   ggb_get_observables records for a step) and norm[kso], on `stream`.  Every pointer must be
+   device-accessible (device memory or mapped host memory); nothing is copied, and no cudaMalloc,
+   cudaFree or allocating library routine is called.
+   Limits: N_l <= 256, N_kso * N_l * ceil(N_r / 32) <= 65536 and N_kso * ceil(N_r / 32) <= 16384;
+   larger sizes return GGB_ERR_ARG.  The partial sums live in fixed arrays inside the library
+   (5.25 MiB, held on every device that loads the library until the process exits) that all calls
+   share: calls that overlap on the GPU (other streams or threads) race, so serialise them.  Each
+   call writes every partial it reads, so nothing has to start at zero.  The first call on a device
+   looks up the arrays' device addresses (cudaGetSymbolAddress) with that device current: make that
+   first call before any stream capture. */
+int ggb_observables_noalloc(const double* x, const double* r, const int* m, int n_l, int n_orb, int n_r,
+                            double* dip, double* acc, double* norm, void* stream);
+
 /* Library version string. */
 const char* ggb_version(void);
 
