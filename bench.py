@@ -38,11 +38,11 @@ import numpy as np  # noqa: E402
 # workloads
 # ---------------------------------------------------------------------------------------------
 
-def workload_runs(name: str, n_t: int, device=None):
-    """Return (runs, precision, description dict)."""
+def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8"):
+    """Return (runs, precision, description dict); ``split`` is the form of the non-FP64 workloads."""
     from ggbtddft_b200 import problems as P
     if name.startswith("ar-ens64"):
-        precision = "fp64" if name.endswith("fp64") else "split_bf16"
+        precision = "fp64" if name.endswith("fp64") else split
         runs = P.argon_ensemble(64, seed=0, n_steps=n_t, device=device)
         ladder = ", ".join(f"{g.n_r}/{g.r_max:.0f}/{g.l_max}" for g in P.ARGON_LADDER)
         return runs, precision, dict(
@@ -51,7 +51,7 @@ def workload_runs(name: str, n_t: int, device=None):
                      " (runs of one grid share W); first steps of the pulse",
             runs=64, n_orb=9, precision=precision, seed=0)
     if name.startswith("hhe-ens256"):
-        precision = "fp64" if name.endswith("fp64") else "split_bf16"
+        precision = "fp64" if name.endswith("fp64") else split
         runs = P.hhe_ensemble(256, seed=0, n_steps=n_t, device=device)
         return runs, precision, dict(
             workload="256-run H/He scan: I log-U[0.5,3]e14, CEP U[0,2pi), lambda U[800,1800] nm, 6-cycle sin^2, "
@@ -59,8 +59,8 @@ def workload_runs(name: str, n_t: int, device=None):
             precision=precision, seed=0)
     if name == "ar-split":
         run = P.config_argon(n_steps=n_t, device=device)
-        return [run], "split_bf16", dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02",
-                                         runs=1, n_r=600, l_max=96, n_orb=9, precision="split_bf16")
+        return [run], split, dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02",
+                                  runs=1, n_r=600, l_max=96, n_orb=9, precision=split)
     if name == "ar-fp64":
         run = P.config_argon(n_steps=n_t, device=device)
         return [run], "fp64", dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02, "
@@ -78,7 +78,13 @@ def workload_runs(name: str, n_t: int, device=None):
 
 
 DEFAULT_WORKLOAD = "ar-ens64"
-SPLIT_PRODUCTS = 5   # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h
+# tensor-core products executed per algorithmic real product, and the peak they run against
+SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (BF16)
+                  "split_int8": 10}   # int8 slice pairs (j, m) with j + m <= 5
+# dense int8 tensor throughput is twice the bf16 throughput on B200 (4.5 vs 2.25 POPS nominal); the
+# int8 roofline takes twice the measured bf16 figure
+TENSOR_PEAK_FACTOR = {"split_bf16": 1.0, "split_int8": 2.0}
+W_BYTES = {"fp64": 16, "split_bf16": 12, "split_int8": 8}   # per complex element of W as streamed
 
 
 # ---------------------------------------------------------------------------------------------
@@ -148,12 +154,13 @@ class ClockSampler:
 def phase_traffic(runs, groups, precision):
     """Algorithmic bytes and flops of each phase of one step, summed over the grid groups.
 
-    radial: W once per group (16 B per complex FP64, 12 B as three BF16 planes per real part) +
+    radial: W once per group (16 B per complex FP64, 12 B as three BF16 planes per real part, 8 B as
+    four int8 slices per real part) +
     orbitals in and out; flops 8 N_r^2 N_l per orbital column (the split products are not counted).
     angular half: orbitals in and out; (#chain GEMMs) x 4 N_l^2 N_r flops per column.
     """
     cb = 16 if precision == "fp64" else 8
-    wb = 16 if precision == "fp64" else 12
+    wb = W_BYTES[precision]
     out = {k: dict(bytes=0.0, flops=0.0) for k in ("radial", "angular_first", "angular_second")}
     for members in groups:
         r0 = runs[members[0]]
@@ -179,7 +186,7 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     n_t = args.warmup + args.steps + 8
-    runs, precision, desc = workload_runs(args.workload, n_t, device="cuda")
+    runs, precision, desc = workload_runs(args.workload, n_t, device="cuda", split=args.precision)
     units_per_step = sum(r.n_orb for r in runs)
     tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
     stream = torch.cuda.Stream()
@@ -248,7 +255,7 @@ def run_ours(args, rank, world, dist):
     # roofline of the dominant kernel
     tf = phase_traffic(runs, tp.groups, precision)
     dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
-    tensor_peak = read_peaks()[1] if precision != "fp64" else None
+    tensor_peak = read_peaks()[1] * TENSOR_PEAK_FACTOR[precision] if precision != "fp64" else None
     kernels = {}
     for k in ("radial", "angular_first", "angular_second"):
         sec = phase_ms[k] / 1e3
@@ -256,18 +263,22 @@ def run_ours(args, rank, world, dist):
                           gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3))
     kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
     rad = kernels["radial"]
-    name = "k_radial_fp64" if precision == "fp64" else "k_radial_tc_persistent (tcgen05, split BF16)"
+    name = {"fp64": "k_radial_fp64", "split_bf16": "k_radial_tc_persistent (tcgen05 kind::f16, split BF16)",
+            "split_int8": "k_radial_i8 (tcgen05 kind::i8, int8 slices, int32 accumulation)"}[precision]
     roofline = dict(bound="hbm", kernel=f"radial propagator ({name})", achieved=rad["gbs"], peak=hbm_peak,
                     unit="GB/s", frac=round(rad["gbs"] / hbm_peak, 4), traffic=None,
                     peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom, kernels=kernels)
     if tensor_peak:
-        # every real product runs as 5 BF16 split products on the tensor cores
+        # every real product runs as several split products on the tensor cores
+        sp = SPLIT_PRODUCTS[precision]
         roofline["tensor_frac_alg"] = round(rad["tflops"] / tensor_peak, 4)
-        roofline["tensor_frac_executed"] = round(SPLIT_PRODUCTS * rad["tflops"] / tensor_peak, 4)
+        roofline["tensor_frac_executed"] = round(sp * rad["tflops"] / tensor_peak, 4)
         if roofline["tensor_frac_executed"] > roofline["frac"]:
-            roofline.update(bound="tensor", achieved=round(SPLIT_PRODUCTS * rad["tflops"], 3), peak=tensor_peak,
-                            unit="TFLOP/s (executed split products)", frac=roofline["tensor_frac_executed"],
-                            peak_kind=f"{peak_kind} bf16_tflops")
+            pk = f"{peak_kind} bf16_tflops" + (" x2 (int8)" if precision == "split_int8" else "")
+            roofline.update(bound="tensor", achieved=round(sp * rad["tflops"], 3), peak=round(tensor_peak, 1),
+                            unit="TFLOP/s (executed split products)" if precision == "split_bf16"
+                            else "TOP/s (executed int8 slice products)",
+                            frac=roofline["tensor_frac_executed"], peak_kind=pk)
     # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU
     fp64_inst = None
     if args.compare_fp64 and (len(runs) > 1 or precision != "fp64"):
@@ -336,6 +347,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=40)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="split_int8", choices=["split_int8", "split_bf16"],
+                    help="form of the split-precision workloads (FP64 workloads end in -fp64)")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")
     ap.add_argument("--compare-fp64", type=int, default=1,
@@ -382,7 +395,7 @@ def main():
         desc["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
         line = dict(metric=metric, value=res["value"], unit="orbital-steps/s", n_gpus=world, steps=args.steps,
                     warmup=args.warmup, ms_per_step=res["ms"] / args.steps, higher_is_better=True,
-                    scaling="weak", vs_baseline=None, dtype="f64" if res["precision"] == "fp64" else "f32+split-bf16",
+                    scaling="weak", vs_baseline=None, dtype={"fp64": "f64", "split_bf16": "f32+split-bf16", "split_int8": "f32+split-int8"}[res["precision"]],
                     data="synthetic (seeded laser parameters; LDA ground state computed at set-up)", config=desc,
                     roofline=res["roofline"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
                     gpu_launches=res["gpu_launches"], fp64_per_instance=res["fp64_per_instance"])

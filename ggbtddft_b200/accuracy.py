@@ -1,16 +1,27 @@
 """Error of the split-precision form against the FP64 form, per result, over a full pulse.
 
-    python -m ggbtddft_b200.accuracy --config argon [--precision split_bf16] [--steps N] [--out report.json]
+    python -m ggbtddft_b200.accuracy --config argon [--precision split_int8] [--steps N] [--frozen]
+                                     [--sensitivity 1e-10] [--out report.json]
 
 Both forms run the same inputs on the GPU (the FP64 form is the one held to the reference to 1e-10).
 Reported: norm drift (max |norm_split - norm_fp64| per orbital), relative L2 error of the total
 dipole and of the total dipole acceleration <cos(theta)/r^2>, and the relative error of every
 harmonic intensity up to the semiclassical cutoff, from the HHG spectrum of the total dipole
 computed with the reference's recipe (spectrum.py).
+
+Conditioning: with Hartree and exchange in the loop the time step feeds the density of one step
+into the potential of the next, and that feedback amplifies small differences (in the FP64 form
+too: a 1e-10 change of the initial orbitals of the argon configuration changes its dipole by tens
+of per cent within a few thousand steps).  ``--sensitivity eps`` runs the FP64 form a second time
+from initial orbitals perturbed by eps (relative, seeded) and reports the same errors for that pair:
+the floor below which no arithmetic other than the identical FP64 sequence can agree with it.
+``--frozen`` runs the same configuration with the potentials frozen at the ground state
+(USE_HARTREE = 0), a linear and well-conditioned propagation on the same grid, orbitals and pulse.
 """
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import time
 from typing import Optional
@@ -40,11 +51,42 @@ def _run(run: P.RunInputs, precision: str, n_steps: int, chunk: int = 4096):
     return obs
 
 
-def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_bf16", n_steps: Optional[int] = None,
-                  e0: Optional[float] = None) -> dict:
+def perturb_orbitals(run: P.RunInputs, eps: float, seed: int = 1) -> P.RunInputs:
+    """Initial orbitals + eps * max|x| * complex Gaussian noise, renormalised per orbital."""
+    rng = np.random.default_rng(seed)
+    x = run.x0 + eps * np.abs(run.x0).max() * (rng.standard_normal(run.x0.shape)
+                                                + 1j * rng.standard_normal(run.x0.shape))
+    x = x / np.sqrt((np.abs(x) ** 2).sum(axis=(0, 2)))[None, :, None]
+    return dataclasses.replace(run, x0=x)
+
+
+def _errors(run, ref, tst, atom, e0):
+    d_ref = S.total_dipole(ref["dipole"], run.l_active, run.m_active, run.occ)
+    d_tst = S.total_dipole(tst["dipole"], run.l_active, run.m_active, run.occ)
+    a_ref = (run.occ[None, :, None] * ref["acceleration"]).real.sum(axis=(0, 1))
+    a_tst = (run.occ[None, :, None] * tst["acceleration"]).real.sum(axis=(0, 1))
+    w, s_ref = S.hhg_spectrum(d_ref, run.dt)
+    _, s_tst = S.hhg_spectrum(d_tst, run.dt)
+    q_cut = S.cutoff_order(IONISATION_POTENTIAL[atom], e0, run.omega0)
+    herr = S.harmonic_errors(s_tst, s_ref, w, run.omega0, q_cut)
+    return dict(norm_drift_max=float(np.abs(tst["norm"] - ref["norm"]).max()),
+                dipole_rel_l2=float(np.linalg.norm(d_tst - d_ref) / np.linalg.norm(d_ref)),
+                acceleration_rel_l2=float(np.linalg.norm(a_tst - a_ref) / np.linalg.norm(a_ref)),
+                harmonic_rel_err=herr.tolist(), odd_harmonic_rel_err_max=float(herr[0::2].max()),
+                harmonic_rel_err_max=float(herr.max()))
+
+
+def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_int8", n_steps: Optional[int] = None,
+                  e0: Optional[float] = None, sensitivity: float = 0.0) -> dict:
     n = run.n_t if n_steps is None else n_steps
     ref = _run(run, "fp64", n)
     tst = _run(run, precision, n)
+    e0 = float(np.abs(run.E).max()) if e0 is None else e0
+    fp64_self = None
+    if sensitivity > 0:
+        pert = _run(perturb_orbitals(run, sensitivity), "fp64", n)
+        fp64_self = dict(eps=sensitivity, **{k: v for k, v in _errors(run, ref, pert, atom, e0).items()
+                                             if k != "harmonic_rel_err"})
     d_ref = S.total_dipole(ref["dipole"], run.l_active, run.m_active, run.occ)
     d_tst = S.total_dipole(tst["dipole"], run.l_active, run.m_active, run.occ)
     a_ref = (run.occ[None, :, None] * ref["acceleration"]).real.sum(axis=(0, 1))
@@ -57,6 +99,7 @@ def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_bf16", n_
     odd = herr[0::2]
     return dict(
         config=run.name, precision=precision, steps=n, dt=run.dt, omega0=run.omega0, cutoff_order=q_cut,
+        use_hartree=int(run.use_hartree), fp64_self_sensitivity=fp64_self,
         seconds=dict(fp64=ref["seconds"], split=tst["seconds"]),
         status=dict(fp64=ref["status"], split=tst["status"]),
         final_norm_fp64=ref["norm"][:, -1].tolist(),
@@ -81,13 +124,18 @@ CONFIGS = {
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="argon", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="split_bf16")
+    ap.add_argument("--precision", default="split_int8")
     ap.add_argument("--steps", type=int, default=None, help="default: the full pulse")
+    ap.add_argument("--frozen", action="store_true", help="potentials frozen at the ground state (USE_HARTREE=0)")
+    ap.add_argument("--sensitivity", type=float, default=0.0,
+                    help="also run FP64 from initial orbitals perturbed by this relative amount")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     atom, builder = CONFIGS[args.config]
     run = builder(n_steps=args.steps, device="cuda")
-    rep = compare_forms(run, atom, args.precision)
+    if args.frozen:
+        run = dataclasses.replace(run, use_hartree=0, name=run.name + "-frozen")
+    rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity)
     line = json.dumps(rep)
     if args.out:
         with open(args.out, "w") as f:

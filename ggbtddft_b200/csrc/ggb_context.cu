@@ -288,6 +288,10 @@ static int prepare(ggb_ctx* ctx) {
     a.n_den = a.hartree_on ? std::min(g.n_har, N_DEN) : 0;
     a.per_l = ctx->dims.per_l;
     a.dt = g.dt;
+    // the FP64 form never raises a norm (its propagators are contractions, rounding is ~1e-15); the
+    // split forms carry a representation error of their operators that may drift it by a few 1e-5
+    // over a long pulse
+    a.norm_tol = ctx->dims.precision == GGB_FP64 ? 1e-6 : 1e-3;
     const int n_g = g.d.n_r + 1;
     a.n_g_fac = (double)(n_g * (n_g + 1)) / 2.0;
     a.r = g.r_d; a.drdx = g.drdx_d; a.P = g.P_d;
@@ -298,7 +302,7 @@ static int prepare(ggb_ctx* ctx) {
     a.chain[0] = c0; a.chain[1] = c1;
     a.chain[2] = c2;
     if (ctx->dims.precision != GGB_FP64) {
-      if ((rc = mixed_prepare(g.mixed, a, g.W_d, ctx->dims.precision, ctx->err))) return rc;
+      if ((rc = mixed_prepare(g.mixed, a, g.W_d, g.x_d, g.y_d, ctx->dims.precision, ctx->err))) return rc;
     }
   }
   // device-side run table
@@ -356,7 +360,7 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
   *out = nullptr;
   if (!dims || !groups || !runs) return GGB_ERR_ARG;
   if (dims->n_groups <= 0 || dims->n_runs <= 0 || dims->n_t <= 0) return GGB_ERR_ARG;
-  if (dims->precision < GGB_FP64 || dims->precision > GGB_SPLIT_TF32) return GGB_ERR_ARG;
+  if (dims->precision < GGB_FP64 || dims->precision > GGB_SPLIT_INT8) return GGB_ERR_ARG;
   ggb_ctx* ctx = new ggb_ctx();
   ctx->dims = *dims;
   cudaGetDevice(&ctx->device);
@@ -405,7 +409,7 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
         (rc = dalloc(ctx, &g.col_run_d, nc)) || (rc = dalloc(ctx, &g.col_m_d, nc)) ||
         (rc = dalloc(ctx, &g.col_occ_d, nc)) || (rc = dalloc(ctx, &g.runs_d, g.runs.size())))
       return bad(rc, "alloc");
-    if (dims->precision == GGB_FP64) {
+    if (dims->precision == GGB_FP64 || dims->precision == GGB_SPLIT_INT8) {
       if ((rc = dalloc(ctx, &g.W_d, nl * nr * nr)) || (rc = dalloc(ctx, &g.x_d, nl * nc * nr)) ||
           (rc = dalloc(ctx, &g.y_d, nl * nc * nr)))
         return bad(rc, "alloc");

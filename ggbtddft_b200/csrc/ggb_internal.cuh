@@ -73,6 +73,7 @@ struct GroupArgs {
   int per_l;
   double dt;
   double n_g_fac;   // N_g (N_g + 1) / 2
+  double norm_tol;  // relative growth of an orbital norm above its initial value that raises ST_NORM_GROWTH
   const double* r;
   const double* drdx;
   const double* P;

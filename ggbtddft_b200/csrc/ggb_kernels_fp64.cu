@@ -141,7 +141,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
     double2* t = xs; xs = ys; ys = t;
   }
 
-  if (rv)
+  if (rv && xout)
     for (int l = warp; l < n_l; l += ANG_WARPS) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * TR + lane];
 
   if (do_obs) {
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
           run.acc_tot[(size_t)k * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
           run.norm[(size_t)k * run.n_t + step] = nrm;
           if (!(nrm == nrm) || isinf(nrm) || !(sx.hi == sx.hi) || !(sz.hi == sz.hi)) atomicOr(g.status, ST_NAN);
-          if (nrm > run.norm0[k] * (1.0 + 1e-6) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
+          if (nrm > run.norm0[k] * (1.0 + g.norm_tol) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
         }
       }
     }

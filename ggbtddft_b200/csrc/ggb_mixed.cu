@@ -577,11 +577,7 @@ static size_t radial_smem(int stages) {
 // host side
 // ---------------------------------------------------------------------------------------------
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
+EncodeTiledFn tensor_map_encoder() {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -595,7 +591,7 @@ static EncodeTiledFn encode_fn() {
 
 // 4-D BF16 tensor (k, rows, plane, l) with a (32, box_rows, planes, 1) box and 64-byte swizzle.
 static bool make_map(CUtensorMap* map, void* base, int k_pad, int rows, int planes, int n_l, int box_rows) {
-  EncodeTiledFn enc = encode_fn();
+  EncodeTiledFn enc = tensor_map_encoder();
   if (!enc) return false;
   cuuint64_t dims[4] = {(cuuint64_t)k_pad, (cuuint64_t)rows, (cuuint64_t)planes, (cuuint64_t)n_l};
   cuuint64_t strides[3] = {(cuuint64_t)k_pad * 2, (cuuint64_t)rows * k_pad * 2,
@@ -640,9 +636,10 @@ static int stages_for(int bn) {
   return s;
 }
 
-int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precision, std::string& err) {
-  if (precision != GGB_SPLIT_BF16) {
-    err = "split_tf32 is not available in this build; use split_bf16";
+int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, double2* x_fp64, double2* y_fp64,
+                  int precision, std::string& err) {
+  if (precision != GGB_SPLIT_BF16 && precision != GGB_SPLIT_INT8) {
+    err = "split_tf32 is not available in this build; use split_int8 or split_bf16";
     return GGB_ERR_ARG;
   }
   m.precision = precision;
@@ -652,10 +649,31 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
   m.bn = pick_bn(nc);
   m.cols_pad = ((nc + m.bn - 1) / m.bn) * m.bn;
   m.stages = stages_for(m.bn);
+  int n_mats = 0;
+  for (int h = 0; h < 2; ++h)
+    for (int o = 0; o < a.chain[h].n_ops; ++o) n_mats = std::max(n_mats, a.chain[h].ops[o].mat + 1);
+  if (precision == GGB_SPLIT_INT8) {
+    // the orbitals stay in the context's FP64 buffers; the observables pass is the FP64 one
+    m.Xd = x_fp64;
+    m.Yd = y_fp64;
+    const int rc = int8_prepare(m, a, W_fp64, n_mats, err);
+    if (rc) return rc;
+    m.ready = true;
+    return GGB_OK;
+  }
   const size_t nx = (size_t)n_l * nc * n_r;
   MX_CK(cudaMalloc(&m.X, nx * sizeof(float2)));
   MX_CK(cudaMalloc(&m.Y, nx * sizeof(float2)));
   MX_CK(cudaMemset(m.Y, 0, nx * sizeof(float2)));
+  int dev = 0, optin = 0;
+  MX_CK(cudaGetDevice(&dev));
+  MX_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (angular_smem_f32(n_l) > (size_t)optin) {
+    err = "N_l too large for the FP32 angular kernel";
+    return GGB_ERR_ARG;
+  }
+  MX_CK(set_max_dynamic_smem((const void*)k_angular_f32<true>, optin));
+  MX_CK(set_max_dynamic_smem((const void*)k_angular_f32<false>, optin));
   const size_t nxs = (size_t)n_l * 4 * m.cols_pad * m.k_pad;
   MX_CK(cudaMalloc(&m.Xsp, nxs * sizeof(__nv_bfloat16)));
   MX_CK(cudaMemset(m.Xsp, 0, nxs * sizeof(__nv_bfloat16)));
@@ -664,10 +682,6 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
   const dim3 tb(32, 8), tg((m.rows_pad + 31) / 32, (m.k_pad + 31) / 32, n_l);
   k_split_w<<<tg, tb>>>(W_fp64, m.Wsp, n_r, m.rows_pad, m.k_pad);
   MX_CK(cudaGetLastError());
-  // chain matrices: count from the chain programs
-  int n_mats = 0;
-  for (int h = 0; h < 2; ++h)
-    for (int o = 0; o < a.chain[h].n_ops; ++o) n_mats = std::max(n_mats, a.chain[h].ops[o].mat + 1);
   const size_t n_mat_el = (size_t)n_mats * a.n_m * n_l * a.ldS;
   MX_CK(cudaMalloc(&m.mats_f, n_mat_el * sizeof(float)));
   k_d2f_real<<<256, 256>>>(a.mats, m.mats_f, n_mat_el);
@@ -684,7 +698,7 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
     MX_CK(cudaMalloc(&m.St, nst * sizeof(__nv_bfloat16)));
     k_build_st<<<512, 256>>>(a.mats, m.St, n_mats, a.n_m, n_l, a.ldS, rows, lk);
     MX_CK(cudaGetLastError());
-    EncodeTiledFn enc = encode_fn();
+    EncodeTiledFn enc = tensor_map_encoder();
     cuuint64_t dims[5] = {(cuuint64_t)lk, (cuuint64_t)rows, S_PLANES, (cuuint64_t)a.n_m, (cuuint64_t)n_mats};
     cuuint64_t strides[4] = {(cuuint64_t)lk * 2, (cuuint64_t)rows * lk * 2, (cuuint64_t)S_PLANES * rows * lk * 2,
                              (cuuint64_t)a.n_m * S_PLANES * rows * lk * 2};
@@ -699,15 +713,6 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
     MX_CK(angular_tc_configure());
     m.angular_tc = true;
   }
-  int dev = 0, optin = 0;
-  MX_CK(cudaGetDevice(&dev));
-  MX_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (angular_smem_f32(n_l) > (size_t)optin) {
-    err = "N_l too large for the FP32 angular kernel";
-    return GGB_ERR_ARG;
-  }
-  MX_CK(set_max_dynamic_smem((const void*)k_angular_f32<true>, optin));
-  MX_CK(set_max_dynamic_smem((const void*)k_angular_f32<false>, optin));
   switch (m.bn) {
     case 16: MX_CK(configure_radial<16>(m.stages)); m.smem = radial_smem<16>(m.stages); break;
     case 32: MX_CK(configure_radial<32>(m.stages)); m.smem = radial_smem<32>(m.stages); break;
@@ -722,6 +727,7 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, int precis
 
 int mixed_load_orbitals(MixedGroup& m, const GroupArgs& a, const double2* x_fp64) {
   if (!m.ready) return GGB_ERR_STATE;
+  if (m.precision == GGB_SPLIT_INT8) return GGB_OK;   // the state is the FP64 buffer itself
   const size_t n = (size_t)a.n_l * a.n_cols * a.n_r;
   k_d2f<<<512, 256>>>(x_fp64, m.X, n);
   return cudaDeviceSynchronize() == cudaSuccess ? GGB_OK : GGB_ERR_CUDA;
@@ -729,6 +735,7 @@ int mixed_load_orbitals(MixedGroup& m, const GroupArgs& a, const double2* x_fp64
 
 int mixed_store_orbitals(MixedGroup& m, const GroupArgs& a, double2* x_fp64) {
   if (!m.ready) return GGB_ERR_STATE;
+  if (m.precision == GGB_SPLIT_INT8) return GGB_OK;
   const size_t n = (size_t)a.n_l * a.n_cols * a.n_r;
   k_f2d<<<512, 256>>>(m.X, x_fp64, n);
   return cudaDeviceSynchronize() == cudaSuccess ? GGB_OK : GGB_ERR_CUDA;
@@ -766,10 +773,22 @@ static void launch_angular_mixed(MixedGroup& m, const GroupArgs& a, int half, co
 }
 
 void mixed_init(MixedGroup& m, const GroupArgs& a, const double2*, cudaStream_t s) {
-  launch_angular_mixed(m, a, 2, m.X, m.X, false, 1, s);
+  if (m.precision == GGB_SPLIT_INT8) launch_angular_fp64(a, 2, m.Xd, nullptr, 1, s);
+  else launch_angular_mixed(m, a, 2, m.X, m.X, false, 1, s);
 }
 
 static void angular_half(MixedGroup& m, const GroupArgs& a, int half, cudaStream_t s) {
+  if (m.precision == GGB_SPLIT_INT8) {
+    if (half == 0) {
+      int8_angular(m, a, 0, m.Xd, m.Xd, s);
+      int8_slice_x(m, a, m.Xd, s);
+    } else {
+      int8_angular(m, a, 1, m.Yd, m.Xd, s);
+      // FP64 density and dipole partial sums of the new orbitals (empty chain, no write-back)
+      launch_angular_fp64(a, 2, m.Xd, nullptr, 1, s);
+    }
+    return;
+  }
   if (m.angular_tc) {
     if (half == 0) {
       launch_angular_tc(m, a, 0, m.X, nullptr, s);
@@ -784,15 +803,20 @@ static void angular_half(MixedGroup& m, const GroupArgs& a, int half, cudaStream
   }
 }
 
+static void radial(MixedGroup& m, const GroupArgs& a, cudaStream_t s) {
+  if (m.precision == GGB_SPLIT_INT8) int8_radial(m, a, s);
+  else launch_radial_tc(m, a, s);
+}
+
 void mixed_step(MixedGroup& m, const GroupArgs& a, cudaStream_t s) {
   angular_half(m, a, 0, s);
-  launch_radial_tc(m, a, s);
+  radial(m, a, s);
   angular_half(m, a, 1, s);
 }
 
 void mixed_phase(MixedGroup& m, const GroupArgs& a, int phase, cudaStream_t s) {
   if (phase == 0) angular_half(m, a, 0, s);
-  if (phase == 1) launch_radial_tc(m, a, s);
+  if (phase == 1) radial(m, a, s);
   if (phase == 2) angular_half(m, a, 1, s);
 }
 
@@ -803,6 +827,7 @@ void mixed_release(MixedGroup& m) {
   cudaFree(m.Wsp);
   cudaFree(m.mats_f);
   cudaFree(m.St);
+  int8_release(m.i8);
   m = MixedGroup();
 }
 

@@ -23,7 +23,7 @@ from .problems import RunInputs
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libggbtddft.so")
 
-PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_tf32": 2}
+PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_tf32": 2, "split_int8": 3}
 COUPLING_IDS = {"P": 0, "FP": 1, "D": 2, "FF": 3}
 RUN_XC_PW92 = 1
 

@@ -33,7 +33,9 @@ typedef struct ggb_ctx ggb_ctx;
 enum {
   GGB_FP64 = 0,        /* complex128 orbitals, FP64 arithmetic: parity form                         */
   GGB_SPLIT_BF16 = 1,  /* complex64 orbitals, 3xBF16 split products on tcgen05, FP32 accumulation    */
-  GGB_SPLIT_TF32 = 2   /* complex64 orbitals, 3xTF32 split products on tcgen05, FP32 accumulation    */
+  GGB_SPLIT_TF32 = 2,  /* reserved: 3xTF32 split products (not built; ggb_create returns GGB_ERR_ARG) */
+  GGB_SPLIT_INT8 = 3   /* complex64 orbitals, four int8 slices per operand on tcgen05 (kind::i8),
+                          exact int32 accumulation: the form that holds the long-pulse error bound   */
 };
 
 /* angular couplings (workingData/hamiltonian/propagatorsL/<dir>):  P 001/001, FP 001/003,
@@ -58,7 +60,7 @@ enum {
 /* A grid group: runs that share the radial grid, N_l and the radial propagators W_l. */
 typedef struct ggb_group_desc {
   int n_r;      /* radial points N_r (any value >= 2; no multiple-of-32 restriction)       */
-  int n_l;      /* angular momenta N_l = l_max + 1 (<= 256)                                 */
+  int n_l;      /* angular momenta N_l = l_max + 1 (<= 220)                                 */
   int n_m;      /* number of azimuthal blocks N_m (m = 0 .. n_m-1)                          */
 } ggb_group_desc;
 
@@ -76,7 +78,7 @@ typedef struct ggb_run_desc {
 typedef struct ggb_dims {
   int n_groups;
   int n_runs;
-  int precision;    /* GGB_FP64 / GGB_SPLIT_BF16 / GGB_SPLIT_TF32                           */
+  int precision;    /* GGB_FP64 / GGB_SPLIT_BF16 / GGB_SPLIT_INT8                           */
   int n_t;          /* capacity of every run's field and observable time series             */
   int per_l;        /* 1: keep dipole/acceleration per (l, orbital) as the reference does   */
 } ggb_dims;

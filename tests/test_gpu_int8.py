@@ -1,0 +1,122 @@
+"""Integer-split form (complex64 orbitals, int8 slices on tcgen05 kind::i8, exact int32 accumulation)
+against the FP64 oracle and the FP64 form."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from ggbtddft_b200 import problems as P
+from ggbtddft_b200.engine import TimePropagation
+from oracle.step_oracle import propagate
+from tests.helpers import rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+# Four base-254 slices per operand row resolve ~2^-31 of the row maximum; products are exact and
+# each result is rounded once to FP32, so one step is accurate to FP32 rounding (a few 1e-7 of the
+# vector norm); over a few dozen steps the FP32 orbital storage dominates (~1e-5 of the dipole).
+TOL_ONE_STEP = 1e-6
+TOL_MULTI = 3e-5
+
+
+def _normalised_random(run, seed=0):
+    rng = np.random.default_rng(seed)
+    n_l, n_r = run.x0.shape[0], run.x0.shape[2]
+    x0 = np.zeros_like(run.x0)
+    v = rng.standard_normal((n_l, n_r)) + 1j * rng.standard_normal((n_l, n_r))
+    x0[:, 0, :] = v / np.linalg.norm(v)
+    return x0
+
+
+@pytest.mark.parametrize("n_r,n_l", [(64, 16), (200, 33), (37, 5), (300, 150)])
+def test_int8_one_step_is_the_radial_product(n_r, n_l):
+    """E = 0 and no Hartree: both angular chains multiply to the identity, so one step is x <- A x.
+    (300, 150) takes the two-M-tile angular chain (N_l > 128)."""
+    run = P.reference_like(n_r, n_l, 4, "H", r_mask=20.0)
+    run = run.with_field(np.zeros(4))
+    x0 = _normalised_random(run)
+    run = dataclasses.replace(run, x0=x0)
+    tp = TimePropagation([run], precision="split_int8")
+    tp.step(1)
+    got = tp.orbitals(0)
+    st, msg = tp.status()
+    tp.close()
+    assert st == 0, msg
+    expect = np.einsum("lba,lkb->lka", run.W, x0)
+    err = np.linalg.norm(got[:, 0] - expect[:, 0]) / np.linalg.norm(expect[:, 0])
+    assert err < TOL_ONE_STEP, err
+
+
+@pytest.mark.parametrize("atom", ["H", "Ne3"])
+def test_split_int8_tracks_fp64_oracle(atom):
+    if atom == "H":
+        run = P.reference_like(64, 32, 48, "H", r_mask=30.0)
+    else:
+        run = P.reference_like(64, 32, 48, "Ne3", r_mask=20.0, dt_as=10.0, perturb=0.05, seed=7)
+    ref = propagate(to_oracle(run))
+    tp = TimePropagation([run], precision="split_int8")
+    tp.step(run.n_t)
+    got = tp.observables(0)
+    st, msg = tp.status()
+    tp.close()
+    assert st == 0, msg
+    assert rel_err(got["norm"], ref["norm"]) < TOL_MULTI
+    assert rel_err(got["dipole"].sum(axis=0), ref["dipole"].sum(axis=0)) < TOL_MULTI
+    assert rel_err(got["acceleration"].sum(axis=0), ref["acceleration"].sum(axis=0)) < TOL_MULTI
+
+
+@pytest.mark.parametrize("atom", ["H", "Ne3"])
+def test_split_int8_norm_follows_fp64_form(atom):
+    """A few hundred steps through a pulse: the int8 norm must follow the FP64 form's norm (which loses
+    probability only to the absorber).  FP32 accumulation on the tensor cores loses ~1e-8 per update
+    in one direction (the split_bf16 form drifts measurably over a few hundred steps); exact integer
+    accumulation must not.  Ne3 adds the Hartree and exchange phases, which repeat nearly the same
+    angle every step: a rotation whose modulus is not 1 would drift the norm steadily."""
+    if atom == "H":
+        run = P.reference_like(128, 24, 400, "H", r_mask=30.0)
+    else:
+        # 100 steps: with the density fed back into the potentials this configuration amplifies any
+        # difference ~1e5-fold per 100 steps beyond that point, in the FP64 form too (a 1e-10 change
+        # of the initial orbitals reaches 1e-3 in the norm by step 200)
+        run = P.reference_like(96, 24, 100, "Ne3", r_mask=20.0, dt_as=10.0, perturb=0.05, seed=5)
+    out = {}
+    for prec in ("fp64", "split_int8"):
+        tp = TimePropagation([run], precision=prec)
+        tp.step(run.n_t)
+        out[prec] = tp.observables(0)["norm"]
+        st, msg = tp.status()
+        tp.close()
+        assert st == 0, (prec, msg)
+    drift = np.abs(out["split_int8"] - out["fp64"]).max()
+    assert drift < 2e-6, drift
+
+
+def test_split_int8_ensemble_group_equals_single_runs():
+    base = P.reference_like(64, 16, 20, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=2)
+    runs = [base.with_field(base.E * s) for s in (1.0, 0.5, 1.5, 0.8)]
+    ens = TimePropagation(runs, precision="split_int8")
+    ens.step(20)
+    for i, r in enumerate(runs):
+        one = TimePropagation([r], precision="split_int8")
+        one.step(20)
+        # integer products are exact: grouping columns changes nothing at all
+        assert np.array_equal(ens.observables(i)["dipole"], one.observables(0)["dipole"])
+        one.close()
+    ens.close()
+
+
+def test_split_int8_scales_each_row():
+    """Every operand row carries its own power-of-two scale: orbitals far from unit norm (x 40, and
+    x 1e-12) are stepped with the same relative accuracy."""
+    run = P.reference_like(64, 16, 4, "H", r_mask=20.0)
+    run = run.with_field(np.zeros(4))
+    x0 = _normalised_random(run, seed=3)
+    expect = np.einsum("lba,lkb->lka", run.W, x0)
+    for s in (40.0, 1e-12):
+        r = dataclasses.replace(run, x0=x0 * s)
+        tp = TimePropagation([r], precision="split_int8")
+        tp.step(1)
+        got = tp.orbitals(0)
+        tp.close()
+        err = np.linalg.norm(got[:, 0] / s - expect[:, 0]) / np.linalg.norm(expect[:, 0])
+        assert err < TOL_ONE_STEP, (s, err)
