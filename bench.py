@@ -85,6 +85,10 @@ SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + 
 # int8 roofline takes twice the measured bf16 figure
 TENSOR_PEAK_FACTOR = {"split_bf16": 1.0, "split_int8": 2.0}
 W_BYTES = {"fp64": 16, "split_bf16": 12, "split_int8": 8}   # per complex element of W as streamed
+# kernels launched per grid group and step: fp64 angular, radial, angular (+ partials), finalize;
+# split_bf16 angular, radial, angular, partials, finalize; split_int8 angular, operand slicing,
+# radial, angular (+ partials), finalize
+LAUNCHES_PER_GROUP_STEP = {"fp64": 4, "split_bf16": 5, "split_int8": 5}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -306,7 +310,8 @@ def run_ours(args, rank, world, dist):
                 e2e=None if e2e_value is None else dict(
                     value=e2e_value, unit="orbital-steps/s", h2d_bytes_per_step=int(h2d / args.steps),
                     d2h_bytes_per_step=int(d2h / args.steps)),
-                gpu_launches=4 * args.steps * len(tp.groups), fp64_per_instance=fp64_inst)
+                gpu_launches=LAUNCHES_PER_GROUP_STEP[precision] * args.steps * len(tp.groups),
+                fp64_per_instance=fp64_inst)
 
 
 def cpu_port_rate(runs, n_steps: int, warmup: int = 1):

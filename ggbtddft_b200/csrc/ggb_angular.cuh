@@ -71,12 +71,15 @@ __device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane
   return d;
 }
 
-__device__ __forceinline__ dd warp_sum_dd(double v) {
+// compensated sum over aligned segments of `seg` lanes (seg = 32: the whole warp)
+__device__ __forceinline__ dd warp_sum_dd(double v, int seg = 32) {
   dd a{v, 0.0};
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    const dd b{__shfl_xor_sync(0xffffffffu, a.hi, o), __shfl_xor_sync(0xffffffffu, a.lo, o)};
-    a = dd_add(a, b);
+    if (o < seg) {
+      const dd b{__shfl_xor_sync(0xffffffffu, a.hi, o), __shfl_xor_sync(0xffffffffu, a.lo, o)};
+      a = dd_add(a, b);
+    }
   }
   return a;
 }
@@ -87,17 +90,23 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Dipole and acceleration partial sums over this tile's radii for every l of one column
-// (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc).
-template <class C, int STRIDE = TR>
-__device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m, int tile, int lane,
-                                 int warp, int n_warps, double rr, double fr2) {
+// Dipole and acceleration partial sums for every l of one column over the radii r0 + lane held by
+// a warp (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc): one
+// partial per g.obs_seg consecutive radii (32 or 16), index (r0 + lane) / g.obs_seg.  Lanes from
+// n_valid on hold no radius.
+// COMPENSATED: double-double sums (the FP64 form, held to 1e-10 of the reference); otherwise plain
+// FP64 sums (the split forms, whose own error is far larger than FP64 summation error).
+template <class C, int STRIDE = TR, bool COMPENSATED = true>
+__device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m, int r0, int lane,
+                                 int warp, int n_warps, double rr, double fr2, int n_valid = TR) {
   const int n_l = g.n_l;
+  const int seg = g.obs_seg;
+  const bool lv = lane < n_valid;
   const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
   const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
   for (int l = warp; l < n_l; l += n_warps) {
     double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (l >= m) {
+    if (l >= m && lv) {
       const double2 xl = to_d2(xs[l * STRIDE + lane]);
       const double2 xu = (l + 1 < n_l) ? to_d2(xs[(l + 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
       const double2 xd = (l >= 1) ? to_d2(xs[(l - 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
@@ -120,9 +129,22 @@ __device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m
       out.w = xl.x * z2.y - xl.y * z2.x;
     }
     // compensated (double-double) reduction over the tile's radii
-    const dd sx = warp_sum_dd(out.x), sy = warp_sum_dd(out.y), sz = warp_sum_dd(out.z), sw = warp_sum_dd(out.w);
-    if (lane == 0) {
-      double4* o = g.obs + 2 * (((size_t)col * n_l + l) * g.n_tiles + tile);
+    dd sx, sy, sz, sw;
+    if (COMPENSATED) {
+      sx = warp_sum_dd(out.x, seg); sy = warp_sum_dd(out.y, seg);
+      sz = warp_sum_dd(out.z, seg); sw = warp_sum_dd(out.w, seg);
+    } else {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        if (o < seg) {
+          out.x += __shfl_xor_sync(0xffffffffu, out.x, o); out.y += __shfl_xor_sync(0xffffffffu, out.y, o);
+          out.z += __shfl_xor_sync(0xffffffffu, out.z, o); out.w += __shfl_xor_sync(0xffffffffu, out.w, o);
+        }
+      }
+      sx = dd{out.x, 0.0}; sy = dd{out.y, 0.0}; sz = dd{out.z, 0.0}; sw = dd{out.w, 0.0};
+    }
+    if (lv && (lane & (seg - 1)) == 0) {
+      double4* o = g.obs + 2 * (((size_t)col * n_l + l) * g.n_tiles + (r0 + lane) / seg);
       o[0] = make_double4(sx.hi, sy.hi, sz.hi, sw.hi);
       o[1] = make_double4(sx.lo, sy.lo, sz.lo, sw.lo);
     }

@@ -268,6 +268,8 @@ k_angular_tc(const __grid_constant__ CUtensorMap tmS, GroupArgs g, AngTcArgs t, 
         tmem_ld16(tmem + lane_base + 128 * mt + p0, re);
         tmem_ld16(tmem + lane_base + 128 * mt + AT_NP + p0, im);
         tmem_ld_wait();
+        tmem_regs_ready(re);
+        tmem_regs_ready(im);
 #pragma unroll
         for (int u = 0; u < 16; ++u) {
           const int p = p0 + u;

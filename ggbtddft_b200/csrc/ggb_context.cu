@@ -24,7 +24,7 @@ namespace {
 
 struct GroupHost {
   ggb_group_desc d{};
-  int n_cols = 0, n_tiles = 0, ldS = 0;
+  int n_cols = 0, n_tiles = 0, obs_seg = TR, ldS = 0;
   std::vector<int> runs;         // ctx run indices
   bool grid_set = false, w_set = false;
   std::vector<double> r, drdx, P;
@@ -74,6 +74,11 @@ struct ggb_ctx {
   int graph_steps = 32;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t cap_stream = nullptr;
+  // one stream per grid group (groups share no buffers, so their steps run concurrently), with the
+  // events that fork them from and join them to the caller's stream
+  std::vector<cudaStream_t> group_streams;
+  std::vector<cudaEvent_t> group_done;
+  cudaEvent_t fork_ev = nullptr;
   std::vector<void*> allocs;
 };
 
@@ -281,7 +286,7 @@ static int prepare(ggb_ctx* ctx) {
     CK(cudaMemcpy(g.coef_d, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice));
 
     GroupArgs& a = g.args;
-    a.n_r = g.d.n_r; a.n_l = n_l; a.n_m = n_m; a.n_cols = g.n_cols; a.n_tiles = g.n_tiles; a.ldS = ldS;
+    a.n_r = g.d.n_r; a.n_l = n_l; a.n_m = n_m; a.n_cols = g.n_cols; a.n_tiles = g.n_tiles; a.obs_seg = g.obs_seg; a.ldS = ldS;
     a.n_runs = (int)g.runs.size();
     a.hartree_on = (g.use_hartree == 1 && g.target_id > 0);
     a.p_hartree = (g.use_hartree == 1 && g.n_har > 1 && g.target_id > 0);
@@ -319,18 +324,43 @@ static int prepare(ggb_ctx* ctx) {
   return GGB_OK;
 }
 
-// one step of every group: angular half 1, radial, angular half 2 (+ partials), finalize
-static int launch_step(ggb_ctx* ctx, cudaStream_t s) {
-  for (GroupHost& g : ctx->groups) {
-    const GroupArgs& a = g.args;
-    if (ctx->dims.precision == GGB_FP64) {
-      launch_angular_fp64(a, 0, g.x_d, g.y_d, 0, s);
-      launch_radial_fp64(a, g.W_d, g.y_d, g.x_d, s);
-      launch_angular_fp64(a, 1, g.x_d, g.x_d, 1, s);
-    } else {
-      mixed_step(g.mixed, a, s);
+// one step of one group: angular half 1, radial, angular half 2 (+ partials), finalize
+static void launch_group_step(ggb_ctx* ctx, GroupHost& g, cudaStream_t s) {
+  const GroupArgs& a = g.args;
+  if (ctx->dims.precision == GGB_FP64) {
+    launch_angular_fp64(a, 0, g.x_d, g.y_d, 0, s);
+    launch_radial_fp64(a, g.W_d, g.y_d, g.x_d, s);
+    launch_angular_fp64(a, 1, g.x_d, g.x_d, 1, s);
+  } else {
+    mixed_step(g.mixed, a, s);
+  }
+  launch_finalize(a, 1, s);
+}
+
+// n steps of every group.  With several groups, each group's steps go to its own stream, forked
+// from and joined back to s by events (inside a graph capture this becomes parallel branches).
+static int launch_steps(ggb_ctx* ctx, cudaStream_t s, int n) {
+  if (n <= 0) return GGB_OK;
+  if (ctx->groups.size() == 1) {
+    for (int i = 0; i < n; ++i) launch_group_step(ctx, ctx->groups[0], s);
+    return GGB_OK;
+  }
+  if (ctx->group_streams.empty()) {
+    ctx->group_streams.assign(ctx->groups.size(), nullptr);
+    ctx->group_done.assign(ctx->groups.size(), nullptr);
+    for (size_t i = 0; i < ctx->groups.size(); ++i) {
+      CK(cudaStreamCreateWithFlags(&ctx->group_streams[i], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&ctx->group_done[i], cudaEventDisableTiming));
     }
-    launch_finalize(a, 1, s);
+    CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+  }
+  CK(cudaEventRecord(ctx->fork_ev, s));
+  for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
+    cudaStream_t gs = ctx->group_streams[gi];
+    CK(cudaStreamWaitEvent(gs, ctx->fork_ev, 0));
+    for (int i = 0; i < n; ++i) launch_group_step(ctx, ctx->groups[gi], gs);
+    CK(cudaEventRecord(ctx->group_done[gi], gs));
+    CK(cudaStreamWaitEvent(s, ctx->group_done[gi], 0));
   }
   return GGB_OK;
 }
@@ -379,7 +409,9 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     g.V.assign(4, std::vector<std::vector<double>>(g.d.n_m));
     g.D.assign(4, std::vector<std::vector<double>>(g.d.n_m));
     g.ang_set.assign(4, std::vector<bool>(g.d.n_m, false));
-    g.n_tiles = (g.d.n_r + TR - 1) / TR;
+    // observables partials: one per 32 radii; the int8 form with N_l > 128 holds 16 radii per CTA
+    g.obs_seg = (dims->precision == GGB_SPLIT_INT8 && g.d.n_l > 128) ? 16 : TR;
+    g.n_tiles = (g.d.n_r + g.obs_seg - 1) / g.obs_seg;
     g.ldS = ((g.d.n_l + 7) / 8) * 8;
   }
   for (int i = 0; i < dims->n_runs; ++i) {
@@ -551,14 +583,18 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream) {
     if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < G; ++i) launch_step(ctx, ctx->cap_stream);
+    const int rc_cap = launch_steps(ctx, ctx->cap_stream, G);
     CK(cudaStreamEndCapture(ctx->cap_stream, &graph));
+    if (rc_cap) {
+      cudaGraphDestroy(graph);
+      return rc_cap;
+    }
     CK(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
     cudaGraphDestroy(graph);
   }
   if (n_steps == 0) return GGB_OK;
   for (int i = 0; i + G <= n_steps; i += G) CK(cudaGraphLaunch(ctx->graph_exec, s));
-  for (int i = 0; i < n_steps % G; ++i) launch_step(ctx, s);
+  if ((rc = launch_steps(ctx, s, n_steps % G))) return rc;
   CK(cudaGetLastError());
   return GGB_OK;
 }
@@ -665,6 +701,9 @@ void ggb_destroy(ggb_ctx* ctx) {
   cudaDeviceSynchronize();
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  for (cudaStream_t gs : ctx->group_streams) cudaStreamDestroy(gs);
+  for (cudaEvent_t e : ctx->group_done) cudaEventDestroy(e);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   for (GroupHost& g : ctx->groups) mixed_release(g.mixed);
   for (void* p : ctx->allocs) cudaFree(p);
   delete ctx;

@@ -60,16 +60,15 @@ __device__ __forceinline__ int row_exponent(double mx) {
 // The four base-254 slices of t, |t| < 126, from one rounding: T = rint(t 254^3) = sum_k s_k 254^(3-k)
 // with balanced digits s_k in [-127, 126].  U = T + 127 (254^3 + 254^2 + 254 + 1) lies in
 // [0, 254^4), so the s_k are its plain base-254 digits minus 127 (unsigned 32-bit arithmetic).
-// Returns s_1 .. s_4 packed in bytes 0 .. 3.
-__device__ __forceinline__ uint32_t slice_int(double t) {
-  uint32_t u = (uint32_t)__double2int_rn(t * 16387064.0) + 2089383045u;
-  const uint32_t d4 = u % 254u;
-  u /= 254u;
-  const uint32_t d3 = u % 254u;
-  u /= 254u;
-  const uint32_t d2 = u % 254u;
-  const uint32_t d1 = u / 254u;
-  return ((d1 - 127u) & 0xffu) | (((d2 - 127u) & 0xffu) << 8) | (((d3 - 127u) & 0xffu) << 16) | ((d4 - 127u) << 24);
+// `t3` is t 254^3.  Each slice is stored as one byte at dst + k * plane.
+template <uint32_t PLANE>
+__device__ __forceinline__ void store_slices(uint8_t* dst, double t3) {
+  const uint32_t u = (uint32_t)__double2int_rn(t3) + 2089383045u;
+  const uint32_t q1 = u / 254u, q2 = q1 / 254u, q3 = q2 / 254u;
+  dst[0] = (uint8_t)(q3 - 127u);
+  dst[PLANE] = (uint8_t)(q2 - q3 * 254u - 127u);
+  dst[2 * PLANE] = (uint8_t)(q1 - q2 * 254u - 127u);
+  dst[3 * PLANE] = (uint8_t)(u - q1 * 254u - 127u);
 }
 
 // four base-254 slices of t (|t| < 127.5): t = s1 + s2/254 + s3/254^2 + s4/254^3 + r, |r| <= 0.5/254^3
@@ -352,6 +351,11 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
           tmem_ld8(d0 + (4 + sidx) * BN + cc, im[sidx]);
         }
         tmem_ld_wait();
+#pragma unroll
+        for (int sidx = 0; sidx < 4; ++sidx) {
+          tmem_regs_ready(re[sidx]);
+          tmem_regs_ready(im[sidx]);
+        }
         if (i < n_r) {
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
@@ -411,19 +415,20 @@ __device__ __forceinline__ uint32_t a8_off(int nrows, int n, int k) {
   return (uint32_t)((k >> 7) * nrows * 128 + n * 128 + chunk * 16 + (k & 15));
 }
 
-// sin and cos of e in FP64: for |e| <= 1 the Maclaurin series through e^15 (sine) and e^16
-// (cosine) in Horner form, truncation below 3e-15 (the phases of a step stay well inside this
-// range); beyond it the library sincos.
+// sin and cos of e in FP64: for |e| <= 1/2 the Maclaurin series through e^11 (sine) and e^12
+// (cosine), evaluated by Estrin's scheme (short dependency chains); truncation below 2e-14 at
+// |e| = 1/2 and far less for the small angles of most phases.  The length-gauge phase r E dt/2 of a
+// step stays below 1/2 for the configurations here (r_max E_0 dt/2 <= 0.4); larger angles take the
+// library sincos.
 __device__ __forceinline__ void sincos_series(double e, double* s, double* c) {
-  if (fabs(e) <= 1.0) {
-    // Estrin's scheme (independent pairs, then powers z^2, z^4) keeps the dependency chains short
+  if (fabs(e) <= 0.5) {
     const double z = e * e, z2 = z * z, z4 = z2 * z2;
     const double s01 = fma(z, -1.0 / 6, 1.0), s23 = fma(z, -1.0 / 5040, 1.0 / 120);
-    const double s45 = fma(z, -1.0 / 39916800, 1.0 / 362880), s67 = fma(z, -1.0 / 1307674368000.0, 1.0 / 6227020800.0);
-    *s = e * fma(z4, fma(z2, s67, s45), fma(z2, s23, s01));
+    const double s45 = fma(z, -1.0 / 39916800, 1.0 / 362880);
+    *s = e * fma(z4, s45, fma(z2, s23, s01));
     const double c01 = fma(z, -1.0 / 2, 1.0), c23 = fma(z, -1.0 / 720, 1.0 / 24);
-    const double c45 = fma(z, -1.0 / 3628800, 1.0 / 40320), c67 = fma(z, -1.0 / 87178291200.0, 1.0 / 479001600.0);
-    *c = fma(z4 * z4, 1.0 / 20922789888000.0, fma(z4, fma(z2, c67, c45), fma(z2, c23, c01)));
+    const double c45 = fma(z, -1.0 / 3628800, 1.0 / 40320);
+    *c = fma(z4 * z2, 1.0 / 479001600.0, fma(z4, c45, fma(z2, c23, c01)));
   } else {
     sincos(e, s, c);
   }
@@ -435,16 +440,13 @@ __device__ __forceinline__ double2 rotd(double2 x, double e) {
   return make_double2(c * x.x + s * x.y, c * x.y - s * x.x);
 }
 
-// x_k(p) into the four slice planes (Re in row p, Im in row NP + p), both scaled by sc
-template <int NP>
-__device__ __forceinline__ void slice_put(uint8_t* xb, uint32_t plane, int p, int k, double2 v, double sc) {
-  const uint32_t sr = slice_int(v.x * sc), si = slice_int(v.y * sc);
-  const uint32_t o_re = a8_off(2 * NP, p, k), o_im = a8_off(2 * NP, NP + p, k);
-#pragma unroll
-  for (int q = 0; q < I8_SLICES; ++q) {
-    xb[q * plane + o_re] = (uint8_t)(sr >> (8 * q));
-    xb[q * plane + o_im] = (uint8_t)(si >> (8 * q));
-  }
+// x_k(p) into the four slice planes: Re in row p, Im in row NP + p (the same swizzle chunk, NP being
+// a multiple of 8); sc3 = 2^e(p) 254^3
+template <int NP, uint32_t PLANE>
+__device__ __forceinline__ void slice_put(uint8_t* xb, int p, int k, double2 v, double sc3) {
+  const uint32_t o = a8_off(2 * NP, p, k);
+  store_slices<PLANE>(xb + o, v.x * sc3);
+  store_slices<PLANE>(xb + o + NP * 128, v.y * sc3);
 }
 
 // One CTA per (orbital column, NP radii): NP = 32 for N_l <= 128 (one M tile of 128 channels),
@@ -463,17 +465,18 @@ __global__ void __launch_bounds__(A8_THREADS, 2)
 k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, const double2* xin, double2* xout) {
   constexpr int NB = 2 * NP;                 // B rows: Re of NP points, then Im
   constexpr int B_TILE = NB * 128;           // one slice plane, one k atom
+  constexpr int K_ATOMS = NP == 32 ? 1 : 2;  // = M tiles = ceil(N_l / 128)
+  constexpr uint32_t XPLANE = K_ATOMS * B_TILE;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ uint64_t full_bar[4], empty_bar[4], acc_bar, xb_bar, drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   __shared__ double pbase[5][NP];
   __shared__ double pnorm2[NP];
-  __shared__ double pscale[NP], pinv[NP];     // 2^e(p) and 2^-e(p) of each point's B rows
+  __shared__ double pscale3[NP], pinv[NP];    // 2^e(p) 254^3 and 2^-e(p) of each point's B rows
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* xb = smem;                                              // 4 planes x k_atoms x B_TILE
-  const uint32_t xplane = (uint32_t)t.k_atoms * B_TILE;
-  uint8_t* sst = smem + (size_t)I8_SLICES * xplane;                 // stages x 16 KB
+  uint8_t* sst = smem + (size_t)I8_SLICES * XPLANE;                 // stages x 16 KB
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_l = g.n_l;
   const int tilesN = (g.n_r + NP - 1) / NP;
@@ -557,7 +560,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     // |Re y_j|, |Im y_j| <= |y| = |x| for every vector of the chain; the margin covers the chain's
     // rounding and the non-orthogonality of the sliced matrices (both ~2^-31)
     const int e = row_exponent(sqrt(pnorm2[threadIdx.x]) * (1.0 + 0x1p-20));
-    pscale[threadIdx.x] = pow2i(e);
+    pscale3[threadIdx.x] = pow2i(e) * 16387064.0;
     pinv[threadIdx.x] = pow2i(-e);
   }
   __syncthreads();
@@ -565,7 +568,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   for (int idx = threadIdx.x; idx < lk * NP; idx += A8_THREADS) {
     const int p = idx / lk, l = idx - p * lk;
     const double2 w = l < n_l ? stg[p * ldf + l] : make_double2(0.0, 0.0);
-    slice_put<NP>(xb, xplane, p, l, w, pscale[p]);
+    slice_put<NP, XPLANE>(xb, p, l, w, pscale3[p]);
   }
   fence_async_smem();
   tc_fence_before();
@@ -623,7 +626,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
                 const uint64_t a = sdesc_kmajor(sa + ko, 128, 2);
 #pragma unroll
                 for (int pb = 0; pb < I8_SLICES - pa; ++pb) {
-                  const uint64_t b = sdesc_kmajor(sxb + pb * xplane + ka * B_TILE + ko, 128, 2);
+                  const uint64_t b = sdesc_kmajor(sxb + pb * XPLANE + ka * B_TILE + ko, 128, 2);
                   const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
                   tc_mma_i8(d0 + (pa + pb) * NB, a, b, idesc, first);
                 }
@@ -642,9 +645,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     const int mt = (t.m_tiles == 2) ? grp : 0;
     const int j = 128 * mt + 32 * q + lane;     // eigen-channel (M row) of this thread
     const int p_begin = (t.m_tiles == 2) ? 0 : A8_PTS * grp;
-    // staging of the last product, [NP][ld] (an odd row length keeps both access patterns free of
-    // bank conflicts)
-    const int ld = t.ld_stage;
+    // staging of the last product, [N_l][NP + 1] (the odd row length keeps both this write, lanes
+    // along l, and the reads below, lanes along the points, free of bank conflicts)
     double2* stage_out = reinterpret_cast<double2*>(smem);
     const uint32_t d0 = tmem + ((uint32_t)(32 * q) << 16) + acc_cols * mt;
     for (int o = 0; o < n_ops; ++o) {
@@ -658,31 +660,54 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       const int pb = op.phase == PH_P ? 1 : op.phase == PH_D ? 2 : 3;
       const bool post_s = last && !SECOND_HALF && ch.post_s && j < n_l;
       const double pj = post_s ? pco[j] : 0.0;
-      // 2^-e_j 254^-3: the S^T row scale and the weight of the integer combination
-      const double scj = pow2i(-t.sexp[((size_t)op.mat * g.n_m + m) * t.rows + j]) * (1.0 / 16387064.0);
-#pragma unroll 1
-      for (int c4 = 0; c4 < A8_PTS / 4; ++c4) {
-        const int p0 = p_begin + 4 * c4;
-        uint32_t re[4][4], im[4][4];
+      const double sj = pow2i(-t.sexp[((size_t)op.mat * g.n_m + m) * t.rows + j]);   // S^T row scale
+      // software pipeline over chunks of 4 points: the next chunk's accumulators are requested
+      // from tensor memory before this chunk is rotated and sliced
+      uint32_t re[4][4], im[4][4];
+      auto tload = [&](int p0) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           tmem_ld4(d0 + s * NB + p0, re[s]);
           tmem_ld4(d0 + s * NB + NP + p0, im[s]);
         }
+      };
+      auto tready = [&]() {
         tmem_ld_wait();
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          tmem_regs_ready(re[s]);
+          tmem_regs_ready(im[s]);
+        }
+      };
+      tload(p_begin);
+      tready();
+#pragma unroll 1
+      for (int c4 = 0; c4 < A8_PTS / 4; ++c4) {
+        const int p0 = p_begin + 4 * c4;
+        // the accumulators hold y 2^(e_j + e_p) 254^3; rotations commute with the scale, and the
+        // next product's slices want y 2^e_p 254^3: one exact power of two in between
+        double2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = make_double2((double)combine_int(re, u) * sj, (double)combine_int(im, u) * sj);
+        if (c4 + 1 < A8_PTS / 4) tload(p0 + 4);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int p = p0 + u;
-          const double sc = scj * pinv[p];
-          double2 v = make_double2((double)combine_int(re, u) * sc, (double)combine_int(im, u) * sc);
-          if (dj != 0.0) v = rotd(v, pbase[pb][p] * dj);
-          if (post_s) v = rotd(v, pbase[4][p] + pj * pbase[2][p]);
+          if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
+          if (post_s) v[u] = rotd(v[u], pbase[4][p] + pj * pbase[2][p]);
           if (!last) {
-            if (j < lk) slice_put<NP>(xb, xplane, p, j, v, pscale[p]);
+            if (j < lk) {
+              const uint32_t o = a8_off(2 * NP, p, j);
+              store_slices<XPLANE>(xb + o, v[u].x);
+              store_slices<XPLANE>(xb + o + NP * 128, v[u].y);
+            }
           } else if (j < n_l) {
-            stage_out[p * ld + j] = v;
+            const double sc = pinv[p] * (1.0 / 16387064.0);
+            stage_out[j * (NP + 1) + p] = make_double2(v[u].x * sc, v[u].y * sc);
           }
         }
+        if (c4 + 1 < A8_PTS / 4) tready();
       }
       tc_fence_before();
       if (!last) {
@@ -699,10 +724,23 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     if (threadIdx.x == 0) atomicOr(g.status, ST_TC_TIMEOUT);
   } else {
     const double2* xs = reinterpret_cast<const double2*>(smem);
-    const int ld = t.ld_stage;
     for (int idx = threadIdx.x; idx < n_l * NP; idx += A8_THREADS) {
       const int l = idx / NP, p = idx - l * NP, r = r0 + p;
-      if (r < g.n_r) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[p * ld + l];
+      if (r < g.n_r) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * (NP + 1) + p];
+    }
+    if (SECOND_HALF) {
+      // FP64 dipole and acceleration partial sums and density multipoles of the new orbitals, from
+      // the staged tile (lanes = points; one partial per NP radii)
+      const int r = r0 + lane;
+      const bool rv = lane < NP && r < g.n_r;
+      const double rr = rv ? g.r[r] : 1.0;
+      const double fr2 = rv ? pow(rr, -2.0) : 0.0;
+      observables_tile<double2, NP + 1, false>(g, xs, col, m, r0, lane, warp, A8_THREADS / 32, rr, fr2, NP);
+      const int n_den = g.n_den > 0 ? g.n_den : 1;   // L = 0 is always needed for the norm
+      for (int L = warp; L < n_den; L += A8_THREADS / 32) {
+        const double d = density_multipole<double2, NP + 1>(L, m, n_l, xs, lane, g.coef, g.n_m);
+        if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
+      }
     }
   }
   tc_fence_before();
@@ -860,15 +898,21 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   }
   // two CTAs per SM: 256 TMEM columns each (NP points x {Re, Im} x 4 accumulators x M tiles) and
   // at most ~110 KB of shared memory each
-  q.np = q.a_m_tiles == 1 ? 32 : 16;
+  q.np = q.a_m_tiles == 1 ? 32 : 16;     // the kernel takes k_atoms = m_tiles = (NP == 32 ? 1 : 2)
   q.a_stages = 4;
   q.a_smem = q.np == 32 ? a8_smem<32>(q.a_k_atoms, q.a_stages) : a8_smem<16>(q.a_k_atoms, q.a_stages);
-  // FP64 staging [NP][ld]: the input tile in the stage buffers, the last product over the operand
-  // planes and stage buffers; an odd row length when it fits
+  // FP64 staging: the input tile [NP][ld] in the stage buffers (an odd ld when it fits), the last
+  // product [N_l][NP + 1] over the operand planes and stage buffers
   q.a_ld = ((size_t)q.np * (n_l | 1) * 16 <= (size_t)q.a_stages * A8_A_TILE) ? (n_l | 1) : n_l;
-  if ((size_t)q.np * q.a_ld * 16 > (size_t)q.a_stages * A8_A_TILE || q.a_smem > 110 * 1024) {
+  if ((size_t)q.np * q.a_ld * 16 > (size_t)q.a_stages * A8_A_TILE ||
+      (size_t)n_l * (q.np + 1) * 16 > q.a_smem - 1024 || q.a_smem > 110 * 1024) {
     err = "int8 angular chain: shared memory";
     return GGB_ERR_ARG;
+  }
+  if (a.obs_seg != q.np) {
+    // the second half writes one observables partial per CTA, so the group's partials are NP radii
+    err = "int8 angular chain: observables partials do not match its tile";
+    return GGB_ERR_STATE;
   }
   const int rows = 128 * q.a_m_tiles, lk = A8_KATOM * q.a_k_atoms;
   q.a_rows = rows;

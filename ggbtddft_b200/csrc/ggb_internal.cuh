@@ -73,7 +73,8 @@ struct GroupArgs {
   int per_l;
   double dt;
   double n_g_fac;   // N_g (N_g + 1) / 2
-  double norm_tol;  // relative growth of an orbital norm above its initial value that raises ST_NORM_GROWTH
+  double norm_tol;
+  int obs_seg;      // radii per observables partial sum (32; 16 for the int8 form when N_l > 128)  // relative growth of an orbital norm above its initial value that raises ST_NORM_GROWTH
   const double* r;
   const double* drdx;
   const double* P;

@@ -32,8 +32,9 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
   extern __shared__ double2 sm[];  // two [N_l][TR] buffers
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int col = blockIdx.x / g.n_tiles;
-  const int tile = blockIdx.x - col * g.n_tiles;
+  const int tiles32 = (g.n_r + TR - 1) / TR;     // this kernel's CTAs cover 32 radii each
+  const int col = blockIdx.x / tiles32;
+  const int tile = blockIdx.x - col * tiles32;
   const int r = tile * TR + lane;
   const bool rv = r < g.n_r;
   const int n_l = g.n_l;
@@ -146,7 +147,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile(g, xs, col, m, tile, lane, warp, ANG_WARPS, rr, fr2);
+    observables_tile(g, xs, col, m, tile * TR, lane, warp, ANG_WARPS, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
     for (int L = warp; L < n_den; L += ANG_WARPS) {
       const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
@@ -159,7 +160,7 @@ size_t angular_smem_fp64(int n_l) { return 2 * (size_t)n_l * TR * sizeof(double2
 
 void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
                          cudaStream_t s) {
-  const dim3 grid(g.n_cols * g.n_tiles), block(ANG_WARPS * 32);
+  const dim3 grid(g.n_cols * ((g.n_r + TR - 1) / TR)), block(ANG_WARPS * 32);
   const size_t smem = angular_smem_fp64(g.n_l);
   k_angular_fp64<<<grid, block, smem, s>>>(g, half, xin, xout, do_obs);
 }

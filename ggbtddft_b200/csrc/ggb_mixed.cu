@@ -143,8 +143,9 @@ k_angular_f32(GroupArgs g, MixArgs mx, int half, const float2* __restrict__ xin,
   extern __shared__ float2 smf[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int col = blockIdx.x / g.n_tiles;
-  const int tile = blockIdx.x - col * g.n_tiles;
+  const int tiles32 = (g.n_r + TR - 1) / TR;     // this kernel's CTAs cover 32 radii each
+  const int col = blockIdx.x / tiles32;
+  const int tile = blockIdx.x - col * tiles32;
   const int r = tile * TR + lane;
   const bool rv = r < g.n_r;
   const int n_l = g.n_l;
@@ -241,7 +242,7 @@ k_angular_f32(GroupArgs g, MixArgs mx, int half, const float2* __restrict__ xin,
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile(g, xs, col, m, tile, lane, warp, ANG_WARPS, rr, fr2);
+    observables_tile(g, xs, col, m, tile * TR, lane, warp, ANG_WARPS, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;
     for (int L = warp; L < n_den; L += ANG_WARPS) {
       const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
@@ -539,6 +540,8 @@ k_radial_tc_persistent(const __grid_constant__ CUtensorMap tmW, const __grid_con
         tmem_ld16(d_re + lane_base + cc, re);
         tmem_ld16(d_im + lane_base + cc, im);
         tmem_ld_wait();
+        tmem_regs_ready(re);
+        tmem_regs_ready(im);
         if (i < n_r) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
@@ -766,7 +769,7 @@ static void launch_radial_tc(MixedGroup& m, const GroupArgs& a, cudaStream_t s) 
 static void launch_angular_mixed(MixedGroup& m, const GroupArgs& a, int half, const float2* xin, float2* xout,
                                  bool split_out, int do_obs, cudaStream_t s) {
   MixArgs mx{m.mats_f, m.k_pad, m.cols_pad, m.Xsp};
-  const dim3 grid(a.n_cols * a.n_tiles), block(ANG_WARPS * 32);
+  const dim3 grid(a.n_cols * ((a.n_r + TR - 1) / TR)), block(ANG_WARPS * 32);
   const size_t smem = angular_smem_f32(a.n_l);
   if (split_out) k_angular_f32<true><<<grid, block, smem, s>>>(a, mx, half, xin, xout, do_obs);
   else k_angular_f32<false><<<grid, block, smem, s>>>(a, mx, half, xin, xout, do_obs);
@@ -783,9 +786,7 @@ static void angular_half(MixedGroup& m, const GroupArgs& a, int half, cudaStream
       int8_angular(m, a, 0, m.Xd, m.Xd, s);
       int8_slice_x(m, a, m.Xd, s);
     } else {
-      int8_angular(m, a, 1, m.Yd, m.Xd, s);
-      // FP64 density and dipole partial sums of the new orbitals (empty chain, no write-back)
-      launch_angular_fp64(a, 2, m.Xd, nullptr, 1, s);
+      int8_angular(m, a, 1, m.Yd, m.Xd, s);   // also the density and dipole partial sums
     }
     return;
   }

@@ -45,13 +45,14 @@ k_obs_partials(const double2* __restrict__ x, const double* __restrict__ r, cons
   g.n_l = n_l;
   g.n_m = NA_MAX_NL;      // the coefficient rows are laid out for m = 0 .. NA_MAX_NL-1
   g.n_tiles = n_tiles;
+  g.obs_seg = TR;
   g.coef = coef;
   g.obs = obs;
   int m = m_of[k];
   if (m < 0 || m > n_l) m = n_l;   // an invalid m contributes nothing (no l satisfies l >= m)
   const double rr = rv ? r[rr_i] : 1.0;
   const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-  observables_tile(g, xs, k, m, tile, lane, warp, NA_WARPS, rr, fr2);
+  observables_tile(g, xs, k, m, tile * TR, lane, warp, NA_WARPS, rr, fr2);
   if (warp == 0) {
     dd s{0.0, 0.0};
     for (int l = m; l < n_l; ++l) {

@@ -24,14 +24,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
+// One test of the phase.  While it is incomplete the thread is suspended (it issues nothing) until
+// the phase completes or ~20 us have passed, so that waiting warps leave the issue slots to the
+// warps that work, and the caller's time limit is still checked regularly.
+constexpr uint32_t WAIT_SUSPEND_NS = 20000;
 __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
+      : "r"(smem_u32(b)), "r"(parity), "r"(WAIT_SUSPEND_NS)
       : "memory");
   return ok != 0;
 }
@@ -101,6 +105,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// The registers a tcgen05.ld writes are valid only after tcgen05.wait::ld, but the asm statements
+// carry no data dependency from the wait to them: pass each through an empty volatile asm after
+// the wait, so that no use of them can be scheduled before it.
+template <int N>
+__device__ __forceinline__ void tmem_regs_ready(uint32_t (&v)[N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) asm volatile("" : "+r"(v[i]));
+}
 
 // Shared-memory matrix descriptor, K-major, with the given swizzle (layout 2 = 128 B, 4 = 64 B):
 // rows of `row_bytes`, 8-row groups `8 * row_bytes` apart.

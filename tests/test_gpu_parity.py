@@ -115,3 +115,24 @@ def test_step_beyond_field_sets_status_not_fault():
     assert st & 2, msg
     assert "beyond" in msg
     tp.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split_int8"])
+def test_several_grid_groups_equal_single_runs(precision):
+    """Runs on three different grids (three groups, stepped on concurrent streams) give exactly the
+    results of each run stepped alone: 70 steps = two graph replays + 6 direct steps."""
+    runs = [P.reference_like(48, 12, 72, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=3),
+            P.reference_like(64, 16, 72, "H", r_mask=20.0),
+            P.reference_like(40, 9, 72, "Ne3", r_mask=12.0, dt_as=10.0, perturb=0.02, seed=4)]
+    ens = TimePropagation(runs, precision=precision)
+    assert len(ens.groups) == 3
+    ens.step(70)
+    st, msg = ens.status()
+    assert st == 0, msg
+    for i, r in enumerate(runs):
+        single = TimePropagation([r], precision=precision)
+        single.step(70)
+        assert np.array_equal(ens.observables(i)["dipole"], single.observables(0)["dipole"])
+        assert np.array_equal(ens.orbitals(i), single.orbitals(0))
+        single.close()
+    ens.close()
