@@ -57,6 +57,13 @@ def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8"):
             workload="256-run H/He scan: I log-U[0.5,3]e14, CEP U[0,2pi), lambda U[800,1800] nm, 6-cycle sin^2, "
                      "dt=0.03; grids N_r 200-800, l_max 32-128 on a ladder", runs=256, n_orb=1,
             precision=precision, seed=0)
+    if name == "ar16-n600":
+        base = P.config_argon(n_steps=n_t, device=device)
+        runs = [base.with_field(base.E * s) for s in np.linspace(0.8, 1.2, 16)]
+        return runs, split, dict(workload="16 argon LDA runs on one grid (N_r=600, r_max=300, l_max=96, dt=0.02; "
+                                          "9 orbitals each), 800 nm 10-cycle sin^2 at 0.8-1.2 x 1.4e14 W/cm^2; "
+                                          "first steps of the pulse", runs=16, n_r=600, l_max=96, n_orb=9,
+                                 precision=split)
     if name == "ar-split":
         run = P.config_argon(n_steps=n_t, device=device)
         return [run], split, dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02",
@@ -80,7 +87,7 @@ def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8"):
 DEFAULT_WORKLOAD = "ar-ens64"
 # tensor-core products executed per algorithmic real product, and the peak they run against
 SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (BF16)
-                  "split_int8": 10}   # int8 slice pairs (j, m) with j + m <= 5
+                  "split_int8": 10}   # int8 slice pairs (j, m), 0-based, with j + m <= 3
 # dense int8 tensor throughput is twice the bf16 throughput on B200 (4.5 vs 2.25 POPS nominal); the
 # int8 roofline takes twice the measured bf16 figure
 TENSOR_PEAK_FACTOR = {"split_bf16": 1.0, "split_int8": 2.0}
@@ -159,23 +166,26 @@ def phase_traffic(runs, groups, precision):
     """Algorithmic bytes and flops of each phase of one step, summed over the grid groups.
 
     radial: W once per group (16 B per complex FP64, 12 B as three BF16 planes per real part, 8 B as
-    four int8 slices per real part) +
-    orbitals in and out; flops 8 N_r^2 N_l per orbital column (the split products are not counted).
-    angular half: orbitals in and out; (#chain GEMMs) x 4 N_l^2 N_r flops per column.
+    four int8 slices per real part) + the orbital operand in (cb B per complex value; the int8 form
+    reads its 12 B of Xr, Xi, -Xi slices) + the result out (cb B); flops 8 N_r^2 N_l per orbital
+    column (the split products are not counted).
+    angular half: orbitals in and out (cb B each); (#chain GEMMs) x 4 N_l^2 N_r flops per column.
+    cb = 16 B for the FP64 and int8 forms (complex128 orbitals), 8 B for the BF16 form.
     """
-    cb = 16 if precision == "fp64" else 8
+    cb = 8 if precision == "split_bf16" else 16
+    xin = 12 if precision == "split_int8" else cb
     wb = W_BYTES[precision]
     out = {k: dict(bytes=0.0, flops=0.0) for k in ("radial", "angular_first", "angular_second")}
     for members in groups:
         r0 = runs[members[0]]
         n_r, n_l = r0.n_r, r0.n_l
         cols = sum(runs[i].n_orb for i in members)
-        x = cb * n_r * n_l * cols
+        elems = n_r * n_l * cols
         n_gemm = 2 + (3 if (r0.use_hartree and r0.target_id > 0 and r0.n_har >= 4) else 0)
-        out["radial"]["bytes"] += wb * n_r * n_r * n_l + 2 * x
+        out["radial"]["bytes"] += wb * n_r * n_r * n_l + (xin + cb) * elems
         out["radial"]["flops"] += 8.0 * n_r * n_r * n_l * cols
         for k in ("angular_first", "angular_second"):
-            out[k]["bytes"] += 2 * x
+            out[k]["bytes"] += 2 * cb * elems
             out[k]["flops"] += n_gemm * 4.0 * n_l * n_l * n_r * cols
     return out
 
@@ -400,7 +410,7 @@ def main():
         desc["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
         line = dict(metric=metric, value=res["value"], unit="orbital-steps/s", n_gpus=world, steps=args.steps,
                     warmup=args.warmup, ms_per_step=res["ms"] / args.steps, higher_is_better=True,
-                    scaling="weak", vs_baseline=None, dtype={"fp64": "f64", "split_bf16": "f32+split-bf16", "split_int8": "f32+split-int8"}[res["precision"]],
+                    scaling="weak", vs_baseline=None, dtype={"fp64": "f64", "split_bf16": "f32+split-bf16", "split_int8": "f64+split-int8"}[res["precision"]],
                     data="synthetic (seeded laser parameters; LDA ground state computed at set-up)", config=desc,
                     roofline=res["roofline"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
                     gpu_launches=res["gpu_launches"], fp64_per_instance=res["fp64_per_instance"])

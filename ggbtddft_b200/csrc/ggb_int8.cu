@@ -7,8 +7,8 @@
 //
 // Representation (Ozaki-style split, base 254):
 //   every operand row (a row of W_l, of a chain matrix S^T, of orbital values) is scaled by a power
-//   of two 2^e that puts its largest |value| in [63.75, 127.5), then cut into four signed 8-bit
-//   slices, each rounded to nearest:
+//   of two 2^e that puts its largest |value| in [63, 126), then cut into four signed 8-bit slices,
+//   rounded to nearest:
 //       v 2^e = a1 + a2 / 254 + a3 / 254^2 + a4 / 254^3 (+ at most 0.5 / 254^3),   |a| <= 127
 //   (base 254, not 256: a remainder in [-0.5, 0.5] times 254 still rounds into [-127, 127]).  A row
 //   is resolved to ~2^-31 of its own maximum.  The constant operators are applied every step, so
@@ -16,13 +16,13 @@
 //   slice buys down.
 //   product: the ten slice pairs (j, m) with j + m <= 3 (0-based; the rest weigh < 254^-4 of the
 //   row maxima and are zero-mean), accumulated exactly in int32 tensor memory, one accumulator per
-//   weight 254^-(j+m); the epilogue combines the four accumulators in FP64, undoes the two row
-//   scales exactly and rounds once, to nearest, to FP32.
+//   weight 254^-(j+m); the epilogue combines the four accumulators exactly (int64), undoes the two
+//   row scales exactly and rounds once to FP64.  The orbitals stay complex128 between products.
 //   int32 range: |a b| <= 127^2, at most 8 products per k and accumulator, K <= 8192: < 2^30.
 //
 //  k_slice_w_i8      W[l][k][i] -> A(i,k) planes [l][8][rows][k] (Wr a1..a4, Wi a1..a4) + exponents
 //  k_build_st_i8     chain matrices -> S^T planes [mat][m][4][rows][lk] + exponents
-//  k_slice_x         orbitals (complex64) -> radial B operand planes (Xr, Xi, -Xi) + exponents
+//  k_slice_x         orbitals (complex128) -> radial B operand planes (Xr, Xi, -Xi) + exponents
 //  k_radial_i8       persistent radial product, kind::i8, 32-byte swizzle, 40 MMAs per 32-wide k block:
 //                      Re_s += Wr_j Xr_m + Wi_j (-Xi)_m,  Im_s += Wr_j Xi_m + Wi_j Xr_m   (j + m = s)
 //  k_angular_i8      the angular chain with int8 operands, exact accumulation and per-point scales
@@ -78,16 +78,6 @@ __device__ __forceinline__ void slice4(double t, int8_t* s) {
     const double a = rint(t);
     s[q] = (int8_t)a;
     t = (t - a) * I8_BASE;
-  }
-}
-// the same in FP32 (t - a is exact; the product by 254 rounds at 2^-24 of a remainder, well below
-// the last slice)
-__device__ __forceinline__ void slice4f(float t, int8_t* s) {
-#pragma unroll
-  for (int q = 0; q < I8_SLICES; ++q) {
-    const float a = rintf(t);
-    s[q] = (int8_t)a;
-    t = (t - a) * (float)I8_BASE;
   }
 }
 

@@ -1,4 +1,4 @@
-"""Integer-split form (complex64 orbitals, int8 slices on tcgen05 kind::i8, exact int32 accumulation)
+"""Integer-split form (complex128 orbitals, int8 slices on tcgen05 kind::i8, exact int32 accumulation)
 against the FP64 oracle and the FP64 form."""
 import dataclasses
 
@@ -12,9 +12,9 @@ from tests.helpers import rel_err, to_oracle
 
 pytestmark = pytest.mark.gpu
 
-# Four base-254 slices per operand row resolve ~2^-31 of the row maximum; products are exact and
-# each result is rounded once to FP32, so one step is accurate to FP32 rounding (a few 1e-7 of the
-# vector norm); over a few dozen steps the FP32 orbital storage dominates (~1e-5 of the dipole).
+# Four base-254 slices per operand row resolve ~2^-31 of the row maximum and the products are exact,
+# so one step is accurate to ~1e-8 of the vector norm; over a few dozen steps of an interacting atom
+# the density feedback amplifies that to ~1e-5 of the dipole.
 TOL_ONE_STEP = 1e-6
 TOL_MULTI = 3e-5
 
