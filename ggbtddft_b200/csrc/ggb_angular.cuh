@@ -72,6 +72,54 @@ __device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane
 }
 
 // compensated sum over aligned segments of `seg` lanes (seg = 32: the whole warp)
+// The seven coefficient rows of one m (CF_CU .. CF_F3 order), contiguous: rows[c * n_l + l].
+// Density multipoles L = 0 .. n_den-1 of one orbital at the radius of this lane: the same terms and
+// literal l ranges as density_multipole, but every l loop is strided over the n_warps warps, and
+// this warp's partial sums are added to d[L] (the caller sums the warps).
+template <class C, int STRIDE>
+__device__ void density_partials(int n_den, int m, int n_l, const C* xs, int lane, const double* rows,
+                                 int warp, int n_warps, double (&d)[N_DEN]) {
+  const double* cu = rows + CF_CU * n_l;
+  const double* cd = rows + CF_CD * n_l;
+  const double* pp = rows + CF_P * n_l;
+  const double* qu = rows + CF_QU * n_l;
+  const double* qd = rows + CF_QD * n_l;
+  const double* p3 = rows + CF_P3 * n_l;
+  const double* f3 = rows + CF_F3 * n_l;
+  auto X = [&](int a, int b) { return xdot<C, STRIDE>(xs, n_l, a, b, lane); };
+  // L = 0
+  for (int lp = m + warp; lp < n_l; lp += n_warps) d[0] += X(lp, lp);
+  if (n_den > 1) {
+    if (warp == 0) d[1] += cf(cu, n_l, m) * X(m + 1, m);
+    for (int lp = m + 1 + warp; lp < n_l - 1; lp += n_warps)
+      d[1] += cf(cu, n_l, lp) * X(lp + 1, lp) + cf(cd, n_l, lp) * X(lp - 1, lp);
+    if (warp == n_warps - 1) d[1] += cf(cd, n_l, n_l - 1) * X(n_l - 2, n_l - 1);
+  }
+  if (n_den > 2) {
+    for (int lp = m + warp; lp < m + 2; lp += n_warps)
+      d[2] += cf(qu, n_l, lp) * X(lp + 2, lp) + cf(pp, n_l, lp) * X(lp, lp);
+    for (int lp = m + 2 + warp; lp < n_l - 2; lp += n_warps)
+      d[2] += cf(qu, n_l, lp) * X(lp + 2, lp) + cf(qd, n_l, lp) * X(lp - 2, lp) + cf(pp, n_l, lp) * X(lp, lp);
+    for (int lp = n_l - 2 + warp; lp < n_l; lp += n_warps)
+      d[2] += cf(qd, n_l, lp) * X(lp - 2, lp) + cf(pp, n_l, lp) * X(lp, lp);
+  }
+  if (n_den > 3) {
+    if (warp == 0) d[3] += cf(p3, n_l, m) * X(m + 1, m) + cf(f3, n_l, m) * X(m + 3, m);
+    for (int lp = m + 1 + warp; lp < m + 3; lp += n_warps)
+      d[3] += cf(p3, n_l, lp - 1) * X(lp - 1, lp) + cf(p3, n_l, lp) * X(lp + 1, lp) + cf(f3, n_l, lp) * X(lp + 3, lp);
+    for (int lp = m + 3 + warp; lp < n_l - 3; lp += n_warps)
+      d[3] += cf(f3, n_l, lp - 3) * X(lp - 3, lp) + cf(p3, n_l, lp - 1) * X(lp - 1, lp) + cf(p3, n_l, lp) * X(lp + 1, lp) +
+              cf(f3, n_l, lp) * X(lp + 3, lp);
+    // the reference's tail loop restarts at N_l - 4 (hartreePotentialDensity.cuh:150)
+    for (int lp = n_l - 4 + warp; lp < n_l - 1; lp += n_warps)
+      d[3] += cf(f3, n_l, lp - 3) * X(lp - 3, lp) + cf(p3, n_l, lp - 1) * X(lp - 1, lp) + cf(p3, n_l, lp) * X(lp + 1, lp);
+    if (warp == n_warps - 1) {
+      const int lp = n_l - 1;
+      d[3] += cf(f3, n_l, lp - 3) * X(lp - 3, lp) + cf(p3, n_l, lp - 1) * X(lp - 1, lp);
+    }
+  }
+}
+
 __device__ __forceinline__ dd warp_sum_dd(double v, int seg = 32) {
   dd a{v, 0.0};
 #pragma unroll
@@ -96,14 +144,17 @@ __device__ __forceinline__ double warp_sum(double v) {
 // n_valid on hold no radius.
 // COMPENSATED: double-double sums (the FP64 form, held to 1e-10 of the reference); otherwise plain
 // FP64 sums (the split forms, whose own error is far larger than FP64 summation error).
+// cu_row, cd_row: the c_u and c_d rows of this m when the caller has staged them (e.g. in shared
+// memory); by default they are read from the group's table.
 template <class C, int STRIDE = TR, bool COMPENSATED = true>
 __device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m, int r0, int lane,
-                                 int warp, int n_warps, double rr, double fr2, int n_valid = TR) {
+                                 int warp, int n_warps, double rr, double fr2, int n_valid = TR,
+                                 const double* cu_row = nullptr, const double* cd_row = nullptr) {
   const int n_l = g.n_l;
   const int seg = g.obs_seg;
   const bool lv = lane < n_valid;
-  const double* cu = g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
-  const double* cd = g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
+  const double* cu = cu_row ? cu_row : g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
+  const double* cd = cd_row ? cd_row : g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
   for (int l = warp; l < n_l; l += n_warps) {
     double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
     if (l >= m && lv) {

@@ -591,7 +591,10 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_i8(128, NB);
-      const uint32_t sxb = smem_u32(xb);
+      // descriptors are formed once; an operand offset only adds (offset >> 4) to the start-address
+      // field (shared-memory offsets stay below 2^18, so the field never carries)
+      const uint64_t bdesc0 = sdesc_kmajor(smem_u32(xb), 128, 2);
+      const uint64_t adesc0 = sdesc_kmajor(smem_u32(sst), 128, 2);
       int it = 0;
       for (int o = 0; o < n_ops; ++o) {
         if (o > 0 && !mbar_wait(&xb_bar, (o - 1) & 1, abort_p)) break;
@@ -599,7 +602,9 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
         bool ok = true;
         for (int mt = 0; mt < t.m_tiles && ok; ++mt) {
           const uint32_t d0 = tmem + acc_cols * mt;
-          for (int ka = 0; ka < t.k_atoms && ok; ++ka)
+          for (int ka = 0; ka < t.k_atoms && ok; ++ka) {
+            const int ksteps = min(A8_KATOM / 32, t.k_steps - ka * (A8_KATOM / 32));
+            const uint64_t bk = bdesc0 + (uint64_t)((ka * B_TILE) >> 4);
             for (int pa = 0; pa < I8_SLICES; ++pa, ++it) {
               const int s = it % t.stages;
               if (!mbar_wait(&full_bar[s], (it / t.stages) & 1, abort_p)) {
@@ -607,22 +612,21 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
                 break;
               }
               tc_fence_after();
-              const uint32_t sa = smem_u32(sst + (size_t)s * A8_A_TILE);
+              const uint64_t ak = adesc0 + (uint64_t)((s * A8_A_TILE) >> 4);
+              const uint32_t acc0 = (ka == 0 && pa == 0) ? 0u : 1u;
 #pragma unroll
               for (int kk = 0; kk < A8_KATOM / 32; ++kk) {
-                const int kstep = ka * (A8_KATOM / 32) + kk;
-                if (kstep >= t.k_steps) break;
-                const uint32_t ko = kk * 32;
-                const uint64_t a = sdesc_kmajor(sa + ko, 128, 2);
+                if (kk >= ksteps) break;
+                const uint64_t a = ak + (uint64_t)(kk * 2);            // 32 bytes
+                const uint32_t acc = kk == 0 ? acc0 : 1u;
 #pragma unroll
-                for (int pb = 0; pb < I8_SLICES - pa; ++pb) {
-                  const uint64_t b = sdesc_kmajor(sxb + pb * XPLANE + ka * B_TILE + ko, 128, 2);
-                  const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
-                  tc_mma_i8(d0 + (pa + pb) * NB, a, b, idesc, first);
-                }
+                for (int pb = 0; pb < I8_SLICES; ++pb)
+                  if (pb < I8_SLICES - pa)
+                    tc_mma_i8(d0 + (pa + pb) * NB, a, bk + (uint64_t)((pb * XPLANE + kk * 32) >> 4), idesc, acc);
               }
               tc_commit(&empty_bar[s]);
             }
+          }
         }
         tc_commit(&acc_bar);
         if (!ok) break;
@@ -721,15 +725,33 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     if (SECOND_HALF) {
       // FP64 dipole and acceleration partial sums and density multipoles of the new orbitals, from
       // the staged tile (lanes = points; one partial per NP radii)
+      // the coefficient rows of this m staged after the tile, then the multipoles computed by all
+      // warps (each literal l loop strided over them) and summed in warp order
+      constexpr int NW = A8_THREADS / 32;
+      double* rows = reinterpret_cast<double*>(smem + (((size_t)n_l * (NP + 1) * 16 + 255) & ~(size_t)255));
+      double* red = rows + COEF_N * n_l;                    // [NW][N_DEN][32]
+      for (int i = threadIdx.x; i < COEF_N * n_l; i += A8_THREADS) {
+        const int c = i / n_l, l = i - c * n_l;
+        rows[i] = g.coef[((size_t)c * g.n_m + m) * n_l + l];
+      }
+      __syncthreads();
       const int r = r0 + lane;
       const bool rv = lane < NP && r < g.n_r;
       const double rr = rv ? g.r[r] : 1.0;
       const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-      observables_tile<double2, NP + 1, false>(g, xs, col, m, r0, lane, warp, A8_THREADS / 32, rr, fr2, NP);
+      observables_tile<double2, NP + 1, false>(g, xs, col, m, r0, lane, warp, NW, rr, fr2, NP, rows + CF_CU * n_l,
+                                               rows + CF_CD * n_l);
       const int n_den = g.n_den > 0 ? g.n_den : 1;   // L = 0 is always needed for the norm
-      for (int L = warp; L < n_den; L += A8_THREADS / 32) {
-        const double d = density_multipole<double2, NP + 1>(L, m, n_l, xs, lane, g.coef, g.n_m);
-        if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
+      double d[N_DEN] = {0.0, 0.0, 0.0, 0.0};
+      density_partials<double2, NP + 1>(n_den, m, n_l, xs, lane, rows, warp, NW, d);
+#pragma unroll
+      for (int L = 0; L < N_DEN; ++L) red[(warp * N_DEN + L) * 32 + lane] = d[L];
+      __syncthreads();
+      if (threadIdx.x < n_den * 32) {
+        const int L = threadIdx.x >> 5, ln = threadIdx.x & 31, rl = r0 + ln;
+        double sum = 0.0;
+        for (int w = 0; w < NW; ++w) sum += red[(w * N_DEN + L) * 32 + ln];
+        if (ln < NP && rl < g.n_r) g.dens[((size_t)col * N_DEN + L) * g.n_r + rl] = sum;
       }
     }
   }
@@ -894,8 +916,11 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   // FP64 staging: the input tile [NP][ld] in the stage buffers (an odd ld when it fits), the last
   // product [N_l][NP + 1] over the operand planes and stage buffers
   q.a_ld = ((size_t)q.np * (n_l | 1) * 16 <= (size_t)q.a_stages * A8_A_TILE) ? (n_l | 1) : n_l;
-  if ((size_t)q.np * q.a_ld * 16 > (size_t)q.a_stages * A8_A_TILE ||
-      (size_t)n_l * (q.np + 1) * 16 > q.a_smem - 1024 || q.a_smem > 110 * 1024) {
+  // the second half's tail: output tile, coefficient rows and the multipoles' warp partials
+  const size_t tail = (((size_t)n_l * (q.np + 1) * 16 + 255) & ~(size_t)255) + (size_t)COEF_N * n_l * 8 +
+                      (size_t)(A8_THREADS / 32) * N_DEN * 32 * 8;
+  if ((size_t)q.np * q.a_ld * 16 > (size_t)q.a_stages * A8_A_TILE || tail > q.a_smem - 1024 ||
+      q.a_smem > 110 * 1024) {
     err = "int8 angular chain: shared memory";
     return GGB_ERR_ARG;
   }
