@@ -591,10 +591,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_i8(128, NB);
-      // descriptors are formed once; an operand offset only adds (offset >> 4) to the start-address
-      // field (shared-memory offsets stay below 2^18, so the field never carries)
-      const uint64_t bdesc0 = sdesc_kmajor(smem_u32(xb), 128, 2);
-      const uint64_t adesc0 = sdesc_kmajor(smem_u32(sst), 128, 2);
+      const uint32_t sxb = smem_u32(xb);
       int it = 0;
       for (int o = 0; o < n_ops; ++o) {
         if (o > 0 && !mbar_wait(&xb_bar, (o - 1) & 1, abort_p)) break;
@@ -602,9 +599,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
         bool ok = true;
         for (int mt = 0; mt < t.m_tiles && ok; ++mt) {
           const uint32_t d0 = tmem + acc_cols * mt;
-          for (int ka = 0; ka < t.k_atoms && ok; ++ka) {
-            const int ksteps = min(A8_KATOM / 32, t.k_steps - ka * (A8_KATOM / 32));
-            const uint64_t bk = bdesc0 + (uint64_t)((ka * B_TILE) >> 4);
+          for (int ka = 0; ka < t.k_atoms && ok; ++ka)
             for (int pa = 0; pa < I8_SLICES; ++pa, ++it) {
               const int s = it % t.stages;
               if (!mbar_wait(&full_bar[s], (it / t.stages) & 1, abort_p)) {
@@ -612,21 +607,22 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
                 break;
               }
               tc_fence_after();
-              const uint64_t ak = adesc0 + (uint64_t)((s * A8_A_TILE) >> 4);
-              const uint32_t acc0 = (ka == 0 && pa == 0) ? 0u : 1u;
+              const uint32_t sa = smem_u32(sst + (size_t)s * A8_A_TILE);
 #pragma unroll
               for (int kk = 0; kk < A8_KATOM / 32; ++kk) {
-                if (kk >= ksteps) break;
-                const uint64_t a = ak + (uint64_t)(kk * 2);            // 32 bytes
-                const uint32_t acc = kk == 0 ? acc0 : 1u;
+                const int kstep = ka * (A8_KATOM / 32) + kk;
+                if (kstep >= t.k_steps) break;
+                const uint32_t ko = kk * 32;
+                const uint64_t a = sdesc_kmajor(sa + ko, 128, 2);
 #pragma unroll
-                for (int pb = 0; pb < I8_SLICES; ++pb)
-                  if (pb < I8_SLICES - pa)
-                    tc_mma_i8(d0 + (pa + pb) * NB, a, bk + (uint64_t)((pb * XPLANE + kk * 32) >> 4), idesc, acc);
+                for (int pb = 0; pb < I8_SLICES - pa; ++pb) {
+                  const uint64_t b = sdesc_kmajor(sxb + pb * XPLANE + ka * B_TILE + ko, 128, 2);
+                  const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
+                  tc_mma_i8(d0 + (pa + pb) * NB, a, b, idesc, first);
+                }
               }
               tc_commit(&empty_bar[s]);
             }
-          }
         }
         tc_commit(&acc_bar);
         if (!ok) break;
