@@ -398,11 +398,12 @@ struct Ang8Args {
   int ld_stage;           // row length of the FP64 staging tiles [NP][ld_stage] (odd when it fits)
 };
 
-// byte offset of (row n, k) in a K-major 128-byte-swizzled plane of nrows rows (one k atom per
-// nrows * 128 bytes)
+// Byte offset of (row n, k) of slice plane 0 in the B operand: per 128-wide k atom, the four slice
+// planes of nrows K-major 128-byte-swizzled rows each, one after the other (plane q at + q nrows 128),
+// so that for one k atom the planes form one operand of 4 nrows rows.
 __device__ __forceinline__ uint32_t a8_off(int nrows, int n, int k) {
   const int chunk = ((k & 127) >> 4) ^ (n & 7);
-  return (uint32_t)((k >> 7) * nrows * 128 + n * 128 + chunk * 16 + (k & 15));
+  return (uint32_t)((k >> 7) * I8_SLICES * nrows * 128 + n * 128 + chunk * 16 + (k & 15));
 }
 
 // sin and cos of e in FP64: for |e| <= 1/2 the Maclaurin series through e^11 (sine) and e^12
@@ -456,7 +457,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   constexpr int NB = 2 * NP;                 // B rows: Re of NP points, then Im
   constexpr int B_TILE = NB * 128;           // one slice plane, one k atom
   constexpr int K_ATOMS = NP == 32 ? 1 : 2;  // = M tiles = ceil(N_l / 128)
-  constexpr uint32_t XPLANE = K_ATOMS * B_TILE;
+  constexpr uint32_t XPLANE = K_ATOMS * B_TILE;  // one slice plane over all k atoms
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ uint64_t full_bar[4], empty_bar[4], acc_bar, xb_bar, drain_bar;
   __shared__ uint32_t tmem_slot;
@@ -558,7 +559,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   for (int idx = threadIdx.x; idx < lk * NP; idx += A8_THREADS) {
     const int p = idx / lk, l = idx - p * lk;
     const double2 w = l < n_l ? stg[p * ldf + l] : make_double2(0.0, 0.0);
-    slice_put<NP, XPLANE>(xb, p, l, w, pscale3[p]);
+    slice_put<NP, B_TILE>(xb, p, l, w, pscale3[p]);
   }
   fence_async_smem();
   tc_fence_before();
@@ -590,7 +591,11 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_i8(128, NB);
+      // one MMA per (S^T slice pa, 32-wide k step): N = (4 - pa) NB rows of the stacked x slice planes
+      // 0 .. 3 - pa, written at TMEM column pa NB, so that its column group pb lands on the
+      // accumulator of weight 254^-(pa + pb)
+      const uint32_t idesc[I8_SLICES] = {idesc_i8(128, 4 * NB), idesc_i8(128, 3 * NB), idesc_i8(128, 2 * NB),
+                                          idesc_i8(128, NB)};
       const uint32_t sxb = smem_u32(xb);
       int it = 0;
       for (int o = 0; o < n_ops; ++o) {
@@ -614,12 +619,9 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
                 if (kstep >= t.k_steps) break;
                 const uint32_t ko = kk * 32;
                 const uint64_t a = sdesc_kmajor(sa + ko, 128, 2);
-#pragma unroll
-                for (int pb = 0; pb < I8_SLICES - pa; ++pb) {
-                  const uint64_t b = sdesc_kmajor(sxb + pb * XPLANE + ka * B_TILE + ko, 128, 2);
-                  const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
-                  tc_mma_i8(d0 + (pa + pb) * NB, a, b, idesc, first);
-                }
+                const uint64_t b = sdesc_kmajor(sxb + ka * I8_SLICES * B_TILE + ko, 128, 2);
+                const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
+                tc_mma_i8(d0 + pa * NB, a, b, idesc[pa], first);
               }
               tc_commit(&empty_bar[s]);
             }
@@ -689,8 +691,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
           if (!last) {
             if (j < lk) {
               const uint32_t o = a8_off(2 * NP, p, j);
-              store_slices<XPLANE>(xb + o, v[u].x);
-              store_slices<XPLANE>(xb + o + NP * 128, v[u].y);
+              store_slices<B_TILE>(xb + o, v[u].x);
+              store_slices<B_TILE>(xb + o + NP * 128, v[u].y);
             }
           } else if (j < n_l) {
             const double sc = pinv[p] * (1.0 / 16387064.0);
