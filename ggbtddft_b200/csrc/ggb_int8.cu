@@ -23,7 +23,8 @@
 //  k_slice_w_i8      W[l][k][i] -> A(i,k) planes [l][8][rows][k] (Wr a1..a4, Wi a1..a4) + exponents
 //  k_build_st_i8     chain matrices -> S^T planes [mat][m][4][rows][lk] + exponents
 //  k_slice_x         orbitals (complex128) -> radial B operand planes (Xr, Xi, -Xi) + exponents
-//  k_radial_i8       persistent radial product, kind::i8, 32-byte swizzle, 40 MMAs per 32-wide k block:
+//  k_radial_i8       persistent radial product, kind::i8, 32-byte swizzle, 16 MMAs per 32-wide k block
+//                    (each covers all x slices m of one W slice j):
 //                      Re_s += Wr_j Xr_m + Wi_j (-Xi)_m,  Im_s += Wr_j Xi_m + Wi_j Xr_m   (j + m = s)
 //  k_angular_i8      the angular chain with int8 operands, exact accumulation and per-point scales
 #include <cuda.h>
@@ -274,7 +275,8 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_i8(R8_BM, BN);
+      const uint32_t idesc[I8_SLICES] = {idesc_i8(R8_BM, 4 * BN), idesc_i8(R8_BM, 3 * BN), idesc_i8(R8_BM, 2 * BN),
+                                          idesc_i8(R8_BM, BN)};
       int it = 0, local = 0;
       for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++local) {
         const int buf = (T::NBUF == 2) ? (local & 1) : 0;
@@ -292,24 +294,22 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
           tc_fence_after();
           const uint32_t sa = smem_u32(smem + (size_t)s * T::STAGE);
           const uint32_t sb = sa + T::A_STAGE;
-          // one 32-wide k block: ten slice pairs (j + m <= 5) of the four real products
+          // one 32-wide k block: for each W slice j, one MMA per real product covers the x slices
+          // m = 0 .. 3 - j at once (the x planes of each kind are contiguous rows), N = (4 - j) BN,
+          // written from accumulator group j on, so that column group m lands on weight 254^-(j+m)
+          const uint64_t xr = sdesc_kmajor(sb, 32, 6);
+          const uint64_t xi = sdesc_kmajor(sb + I8_SLICES * T::B_PLANE, 32, 6);
+          const uint64_t xn = sdesc_kmajor(sb + 2 * I8_SLICES * T::B_PLANE, 32, 6);
 #pragma unroll
           for (int j = 0; j < I8_SLICES; ++j) {
             const uint64_t wr = sdesc_kmajor(sa + j * T::A_PLANE, 32, 6);
             const uint64_t wi = sdesc_kmajor(sa + (I8_SLICES + j) * T::A_PLANE, 32, 6);
-#pragma unroll
-            for (int mm = 0; mm < I8_SLICES - j; ++mm) {
-              const int sidx = j + mm;                         // weight 2^-7 sidx
-              const uint64_t xr = sdesc_kmajor(sb + mm * T::B_PLANE, 32, 6);
-              const uint64_t xi = sdesc_kmajor(sb + (I8_SLICES + mm) * T::B_PLANE, 32, 6);
-              const uint64_t xn = sdesc_kmajor(sb + (2 * I8_SLICES + mm) * T::B_PLANE, 32, 6);
-              const uint32_t dre = d0 + sidx * BN, dim = d0 + (4 + sidx) * BN;
-              const uint32_t first = (kb == 0 && j == 0) ? 0u : 1u;
-              tc_mma_i8(dre, wr, xr, idesc, first);
-              tc_mma_i8(dre, wi, xn, idesc, 1u);
-              tc_mma_i8(dim, wr, xi, idesc, first);
-              tc_mma_i8(dim, wi, xr, idesc, 1u);
-            }
+            const uint32_t dre = d0 + j * BN, dim = d0 + (4 + j) * BN;
+            const uint32_t first = (kb == 0 && j == 0) ? 0u : 1u;
+            tc_mma_i8(dre, wr, xr, idesc[j], first);
+            tc_mma_i8(dre, wi, xn, idesc[j], 1u);
+            tc_mma_i8(dim, wr, xi, idesc[j], first);
+            tc_mma_i8(dim, wi, xr, idesc[j], 1u);
           }
           tc_commit(&empty_bar[s]);
         }
