@@ -626,6 +626,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
               tc_commit(&empty_bar[s]);
             }
         }
+        // one commit for all M tiles: every tile's products read the whole operand, which the
+        // epilogue overwrites with the next product's
         tc_commit(&acc_bar);
         if (!ok) break;
       }
@@ -641,12 +643,22 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     // along l, and the reads below, lanes along the points, free of bank conflicts)
     double2* stage_out = reinterpret_cast<double2*>(smem);
     const uint32_t d0 = tmem + ((uint32_t)(32 * q) << 16) + acc_cols * mt;
+    // a warp whose 32 channels are all padding (j >= N_l) does no work: its rows of the next
+    // operand stay as the fill left them (zero), and the next product's S^T columns there are zero
+    const bool live = 128 * mt + 32 * q < n_l;
     for (int o = 0; o < n_ops; ++o) {
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_bar, o & 1, abort_p));
       tc_fence_after();
       if (!ok) break;
       const ChainOp op = ch.ops[o];
       const bool last = (o == n_ops - 1);
+      if (!live) {
+        if (!last) {
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&xb_bar);
+        }
+        continue;
+      }
       const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
       const double dj = (op.phase != PH_NONE && j >= m && j < n_l) ? Dv[j] : 0.0;
       const int pb = op.phase == PH_P ? 1 : op.phase == PH_D ? 2 : 3;
