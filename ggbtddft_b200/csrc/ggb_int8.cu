@@ -734,34 +734,71 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     }
     if (SECOND_HALF) {
       // FP64 dipole and acceleration partial sums and density multipoles of the new orbitals, from
-      // the staged tile (lanes = points; one partial per NP radii)
-      // the coefficient rows of this m staged after the tile, then the multipoles computed by all
-      // warps (each literal l loop strided over them) and summed in warp order
+      // the staged tile, with the coefficient rows of this m staged after it.
       constexpr int NW = A8_THREADS / 32;
+      constexpr int LG = 32 / NP;        // lane groups per warp: lane = (point, l-loop group)
+      constexpr int NG = NW * LG;        // groups that stride the density's l loops
       double* rows = reinterpret_cast<double*>(smem + (((size_t)n_l * (NP + 1) * 16 + 255) & ~(size_t)255));
-      double* red = rows + COEF_N * n_l;                    // [NW][N_DEN][32]
+      double* red = rows + COEF_N * n_l;                    // [NG][N_DEN][NP]
+      double* prr = red + NG * N_DEN * NP;                  // [2][NP]: r and r^-2 of each point (0 past N_r)
       for (int i = threadIdx.x; i < COEF_N * n_l; i += A8_THREADS) {
         const int c = i / n_l, l = i - c * n_l;
         rows[i] = g.coef[((size_t)c * g.n_m + m) * n_l + l];
       }
+      if (threadIdx.x < NP) {
+        const int r = r0 + threadIdx.x;
+        const double rr = r < g.n_r ? g.r[r] : 0.0;
+        prr[threadIdx.x] = rr;
+        prr[NP + threadIdx.x] = r < g.n_r ? pow(rr, -2.0) : 0.0;
+      }
       __syncthreads();
-      const int r = r0 + lane;
-      const bool rv = lane < NP && r < g.n_r;
-      const double rr = rv ? g.r[r] : 1.0;
-      const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-      observables_tile<double2, NP + 1, false>(g, xs, col, m, r0, lane, warp, NW, rr, fr2, NP, rows + CF_CU * n_l,
-                                               rows + CF_CD * n_l);
+      // dipole and acceleration: one thread per l, summing this CTA's NP radii in order (the same
+      // terms as observables_tile; one partial per (l, NP radii))
+      for (int l = threadIdx.x; l < n_l; l += A8_THREADS) {
+        double sx = 0.0, sy = 0.0, sz = 0.0, sw = 0.0;
+        if (l >= m) {
+          const double c_u = rows[CF_CU * n_l + l], c_d = rows[CF_CD * n_l + l];
+          const bool has_u = l + 1 < n_l, has_d = l >= 1;
+          for (int p = 0; p < NP; ++p) {
+            const double rr = prr[p], fr2 = prr[NP + p];
+            const double2 xl = xs[l * (NP + 1) + p];
+            const double2 xu = has_u ? xs[(l + 1) * (NP + 1) + p] : make_double2(0.0, 0.0);
+            const double2 xd = has_d ? xs[(l - 1) * (NP + 1) + p] : make_double2(0.0, 0.0);
+            double2 z1, z2;
+            if (l == m) {
+              z1 = make_double2(rr * c_u * xu.x, rr * c_u * xu.y);
+              z2 = make_double2(fr2 * c_u * xu.x, fr2 * c_u * xu.y);
+            } else if (l == n_l - 1) {
+              z1 = make_double2(rr * c_d * xd.x, rr * c_d * xd.y);
+              z2 = make_double2(fr2 * c_d * xd.x, fr2 * c_d * xd.y);
+            } else {
+              z1 = make_double2(rr * c_u * xu.x + rr * c_d * xd.x, rr * c_u * xu.y + rr * c_d * xd.y);
+              z2 = make_double2(fr2 * (c_u * xu.x + c_d * xd.x), fr2 * (c_u * xu.y + c_d * xd.y));
+            }
+            sx += xl.x * z1.x + xl.y * z1.y;
+            sy += xl.x * z1.y - xl.y * z1.x;
+            sz += xl.x * z2.x + xl.y * z2.y;
+            sw += xl.x * z2.y - xl.y * z2.x;
+          }
+        }
+        double4* o = g.obs + 2 * (((size_t)col * n_l + l) * g.n_tiles + r0 / NP);
+        o[0] = make_double4(sx, sy, sz, sw);
+        o[1] = make_double4(0.0, 0.0, 0.0, 0.0);
+      }
+      // density multipoles: every lane works (point lane % NP), the literal l loops strided over the
+      // NG lane groups, then the groups summed in order
       const int n_den = g.n_den > 0 ? g.n_den : 1;   // L = 0 is always needed for the norm
+      const int pt = lane % NP, gi = warp * LG + lane / NP;
       double d[N_DEN] = {0.0, 0.0, 0.0, 0.0};
-      density_partials<double2, NP + 1>(n_den, m, n_l, xs, lane, rows, warp, NW, d);
+      density_partials<double2, NP + 1>(n_den, m, n_l, xs, pt, rows, gi, NG, d);
 #pragma unroll
-      for (int L = 0; L < N_DEN; ++L) red[(warp * N_DEN + L) * 32 + lane] = d[L];
+      for (int L = 0; L < N_DEN; ++L) red[(gi * N_DEN + L) * NP + pt] = d[L];
       __syncthreads();
-      if (threadIdx.x < n_den * 32) {
-        const int L = threadIdx.x >> 5, ln = threadIdx.x & 31, rl = r0 + ln;
+      if (threadIdx.x < n_den * NP) {
+        const int L = threadIdx.x / NP, pp = threadIdx.x - L * NP, rl = r0 + pp;
         double sum = 0.0;
-        for (int w = 0; w < NW; ++w) sum += red[(w * N_DEN + L) * 32 + ln];
-        if (ln < NP && rl < g.n_r) g.dens[((size_t)col * N_DEN + L) * g.n_r + rl] = sum;
+        for (int w = 0; w < NG; ++w) sum += red[(w * N_DEN + L) * NP + pp];
+        if (rl < g.n_r) g.dens[((size_t)col * N_DEN + L) * g.n_r + rl] = sum;
       }
     }
   }
@@ -928,7 +965,7 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   q.a_ld = ((size_t)q.np * (n_l | 1) * 16 <= (size_t)q.a_stages * A8_A_TILE) ? (n_l | 1) : n_l;
   // the second half's tail: output tile, coefficient rows and the multipoles' warp partials
   const size_t tail = (((size_t)n_l * (q.np + 1) * 16 + 255) & ~(size_t)255) + (size_t)COEF_N * n_l * 8 +
-                      (size_t)(A8_THREADS / 32) * N_DEN * 32 * 8;
+                      (size_t)(A8_THREADS / 32) * N_DEN * 32 * 8 + 2 * (size_t)q.np * 8;
   if ((size_t)q.np * q.a_ld * 16 > (size_t)q.a_stages * A8_A_TILE || tail > q.a_smem - 1024 ||
       q.a_smem > 110 * 1024) {
     err = "int8 angular chain: shared memory";
