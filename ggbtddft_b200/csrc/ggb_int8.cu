@@ -5,20 +5,20 @@
 // hundred updates per orbital value: the norm then decays geometrically (measured: ~1.4e-8 per
 // update, 2.4 % over the 8,826 steps of the hydrogen pulse).  Integer products accumulate exactly.
 //
-// Representation (Ozaki-style split, base 254):
+// Representation (Ozaki-style split, base 256):
 //   every operand row (a row of W_l, of a chain matrix S^T, of orbital values) is scaled by a power
-//   of two 2^e that puts its largest |value| in [63, 126), then cut into four signed 8-bit slices,
-//   rounded to nearest:
-//       v 2^e = a1 + a2 / 254 + a3 / 254^2 + a4 / 254^3 (+ at most 0.5 / 254^3),   |a| <= 127
-//   (base 254, not 256: a remainder in [-0.5, 0.5] times 254 still rounds into [-127, 127]).  A row
-//   is resolved to ~2^-31 of its own maximum.  The constant operators are applied every step, so
-//   their representation error is a fixed non-unitarity that compounds: it is what the fourth
+//   of two 2^e that puts its largest |value| in [63, 126), rounded once to T = rint(v 2^e 2^24)
+//   (|T| < 2^31) and cut into its four balanced base-256 digits, the bytes of T + 0x80808080 each
+//   less 128 (an int8 in [-128, 127]):
+//       v 2^e = a1 + a2 2^-8 + a3 2^-16 + a4 2^-24 (+ at most 2^-25)
+//   A row is resolved to ~2^-31 of its own maximum.  The constant operators are applied every step,
+//   so their representation error is a fixed non-unitarity that compounds: it is what the fourth
 //   slice buys down.
-//   product: the ten slice pairs (j, m) with j + m <= 3 (0-based; the rest weigh < 254^-4 of the
+//   product: the ten slice pairs (j, m) with j + m <= 3 (0-based; the rest weigh < 2^-32 of the
 //   row maxima and are zero-mean), accumulated exactly in int32 tensor memory, one accumulator per
-//   weight 254^-(j+m); the epilogue combines the four accumulators exactly (int64), undoes the two
-//   row scales exactly and rounds once to FP64.  The orbitals stay complex128 between products.
-//   int32 range: |a b| <= 127^2, at most 8 products per k and accumulator, K <= 8192: < 2^30.
+//   weight 2^-8(j+m); the epilogue combines the four accumulators exactly (int64 shifts), undoes the
+//   two row scales exactly and rounds once to FP64.  The orbitals stay complex128 between products.
+//   int32 range: |a b| <= 2^14, at most 8 products per k and accumulator, K <= 8192: <= 2^30.
 //
 //  k_slice_w_i8      W[l][k][i] -> A(i,k) planes [l][8][rows][k] (Wr a1..a4, Wi a1..a4) + exponents
 //  k_build_st_i8     chain matrices -> S^T planes [mat][m][4][rows][lk] + exponents
@@ -45,7 +45,6 @@ constexpr int I8_SLICES = 4;
 // slicing
 // ---------------------------------------------------------------------------------------------
 
-constexpr double I8_BASE = 254.0;
 
 // exponent e with max 2^e in [63, 126) (0 for an all-zero row): with max = f 2^E, f in [0.5, 1),
 // f 2^7 lies in [64, 126) unless f >= 126 / 128, and then f 2^6 lies in [63, 64).  Below 126 the
@@ -58,28 +57,25 @@ __device__ __forceinline__ int row_exponent(double mx) {
   return min(1000, 7 - ex - (f >= 126.0 / 128.0 ? 1 : 0));
 }
 
-// The four base-254 slices of t, |t| < 126, from one rounding: T = rint(t 254^3) = sum_k s_k 254^(3-k)
-// with balanced digits s_k in [-127, 126].  U = T + 127 (254^3 + 254^2 + 254 + 1) lies in
-// [0, 254^4), so the s_k are its plain base-254 digits minus 127 (unsigned 32-bit arithmetic).
-// `t3` is t 254^3.  Each slice is stored as one byte at dst + k * plane.
+// The four balanced base-256 digits of T = rint(t3), t3 = t 2^24 with |t| < 126 (|T| < 2^31): the
+// bytes of (T + 0x80808080) xor 0x80808080, each an int8 in [-128, 127], T = sum_k a_k 2^(8(3-k)).
+__device__ __forceinline__ uint32_t slice_word(double t3) {
+  return ((uint32_t)__double2int_rn(t3) + 0x80808080u) ^ 0x80808080u;
+}
+// the four slices of t3 stored one byte at dst + k * PLANE, most significant first
 template <uint32_t PLANE>
 __device__ __forceinline__ void store_slices(uint8_t* dst, double t3) {
-  const uint32_t u = (uint32_t)__double2int_rn(t3) + 2089383045u;
-  const uint32_t q1 = u / 254u, q2 = q1 / 254u, q3 = q2 / 254u;
-  dst[0] = (uint8_t)(q3 - 127u);
-  dst[PLANE] = (uint8_t)(q2 - q3 * 254u - 127u);
-  dst[2 * PLANE] = (uint8_t)(q1 - q2 * 254u - 127u);
-  dst[3 * PLANE] = (uint8_t)(u - q1 * 254u - 127u);
+  const uint32_t v = slice_word(t3);
+  dst[0] = (uint8_t)(v >> 24);
+  dst[PLANE] = (uint8_t)(v >> 16);
+  dst[2 * PLANE] = (uint8_t)(v >> 8);
+  dst[3 * PLANE] = (uint8_t)v;
 }
-
-// four base-254 slices of t (|t| < 127.5): t = s1 + s2/254 + s3/254^2 + s4/254^3 + r, |r| <= 0.5/254^3
+// the four slices of t (|t| < 126) as int8 values, most significant first
 __device__ __forceinline__ void slice4(double t, int8_t* s) {
+  const uint32_t v = slice_word(t * 16777216.0);
 #pragma unroll
-  for (int q = 0; q < I8_SLICES; ++q) {
-    const double a = rint(t);
-    s[q] = (int8_t)a;
-    t = (t - a) * I8_BASE;
-  }
+  for (int q = 0; q < I8_SLICES; ++q) s[q] = (int8_t)(uint8_t)(v >> (24 - 8 * q));
 }
 
 // row maxima of A(i,k) = W[l][k][i] over k (re and im)
@@ -186,10 +182,10 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 __device__ __forceinline__ double pow2i(int k) {
   return k < -1022 ? 0.0 : __longlong_as_double((long long)(k + 1023) << 52);
 }
-// sum_s D_s 254^(3-s) of the four int32 accumulators of column u, exactly (|D_s| < 2^30: < 2^55)
+// sum_s D_s 2^(8(3-s)) of the four int32 accumulators of column u, exactly (|D_s| <= 2^30: < 2^55)
 template <int W>
 __device__ __forceinline__ long long combine_int(const uint32_t (&d)[4][W], int u) {
-  return (long long)(int)d[0][u] * 16387064LL + (long long)(int)d[1][u] * 64516LL + (long long)(int)d[2][u] * 254LL +
+  return (long long)(int)d[0][u] * 16777216LL + (long long)(int)d[1][u] * 65536LL + (long long)(int)d[2][u] * 256LL +
          (long long)(int)d[3][u];
 }
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
@@ -296,7 +292,7 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
           const uint32_t sb = sa + T::A_STAGE;
           // one 32-wide k block: for each W slice j, one MMA per real product covers the x slices
           // m = 0 .. 3 - j at once (the x planes of each kind are contiguous rows), N = (4 - j) BN,
-          // written from accumulator group j on, so that column group m lands on weight 254^-(j+m)
+          // written from accumulator group j on, so that column group m lands on weight 2^-8(j+m)
           const uint64_t xr = sdesc_kmajor(sb, 32, 6);
           const uint64_t xi = sdesc_kmajor(sb + I8_SLICES * T::B_PLANE, 32, 6);
           const uint64_t xn = sdesc_kmajor(sb + 2 * I8_SLICES * T::B_PLANE, 32, 6);
@@ -351,7 +347,7 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
           for (int u = 0; u < 8; ++u) {
             const int c = c0 + cc + u;
             if (c < n_cols) {
-              const double sc = pow2i(-ew - xexp[(size_t)l * cols_pad + c]) * (1.0 / 16387064.0);
+              const double sc = pow2i(-ew - xexp[(size_t)l * cols_pad + c] - 24);
               Y[((size_t)l * n_cols + c) * n_r + i] =
                   make_double2((double)combine_int(re, u) * sc, (double)combine_int(im, u) * sc);
             }
@@ -432,7 +428,7 @@ __device__ __forceinline__ double2 rotd(double2 x, double e) {
 }
 
 // x_k(p) into the four slice planes: Re in row p, Im in row NP + p (the same swizzle chunk, NP being
-// a multiple of 8); sc3 = 2^e(p) 254^3
+// a multiple of 8); sc3 = 2^e(p) 2^24
 template <int NP, uint32_t PLANE>
 __device__ __forceinline__ void slice_put(uint8_t* xb, int p, int k, double2 v, double sc3) {
   const uint32_t o = a8_off(2 * NP, p, k);
@@ -464,7 +460,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   __shared__ int abort_flag;
   __shared__ double pbase[5][NP];
   __shared__ double pnorm2[NP];
-  __shared__ double pscale3[NP], pinv[NP];    // 2^e(p) 254^3 and 2^-e(p) of each point's B rows
+  __shared__ double pscale3[NP], pinv[NP];    // 2^e(p) 2^24 and 2^-e(p) of each point's B rows
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* xb = smem;                                              // 4 planes x k_atoms x B_TILE
   uint8_t* sst = smem + (size_t)I8_SLICES * XPLANE;                 // stages x 16 KB
@@ -477,7 +473,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   const RunDev run = g.runs[g.col_run[col]];
   const Chain& ch = g.chain[SECOND_HALF ? 1 : 0];
   const int n_ops = ch.n_ops;
-  const int acc_cols = 4 * NB;                // per M tile: weights 254^0 .. 254^-3
+  const int acc_cols = 4 * NB;                // per M tile: weights 2^0 .. 2^-24
   int step = *g.step;
   if (step >= run.n_t) step = run.n_t - 1;
   const double hdt = 0.5 * g.dt;
@@ -551,7 +547,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     // |Re y_j|, |Im y_j| <= |y| = |x| for every vector of the chain; the margin covers the chain's
     // rounding and the non-orthogonality of the sliced matrices (both ~2^-31)
     const int e = row_exponent(sqrt(pnorm2[threadIdx.x]) * (1.0 + 0x1p-20));
-    pscale3[threadIdx.x] = pow2i(e) * 16387064.0;
+    pscale3[threadIdx.x] = pow2i(e + 24);
     pinv[threadIdx.x] = pow2i(-e);
   }
   __syncthreads();
@@ -593,7 +589,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     if (lane == 0) {
       // one MMA per (S^T slice pa, 32-wide k step): N = (4 - pa) NB rows of the stacked x slice planes
       // 0 .. 3 - pa, written at TMEM column pa NB, so that its column group pb lands on the
-      // accumulator of weight 254^-(pa + pb)
+      // accumulator of weight 2^-8(pa + pb)
       const uint32_t idesc[I8_SLICES] = {idesc_i8(128, 4 * NB), idesc_i8(128, 3 * NB), idesc_i8(128, 2 * NB),
                                           idesc_i8(128, NB)};
       const uint32_t sxb = smem_u32(xb);
@@ -688,8 +684,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
 #pragma unroll 1
       for (int c4 = 0; c4 < A8_PTS / 4; ++c4) {
         const int p0 = p_begin + 4 * c4;
-        // the accumulators hold y 2^(e_j + e_p) 254^3; rotations commute with the scale, and the
-        // next product's slices want y 2^e_p 254^3: one exact power of two in between
+        // the accumulators hold y 2^(e_j + e_p) 2^24; rotations commute with the scale, and the
+        // next product's slices want y 2^e_p 2^24: one exact power of two in between
         double2 v[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -707,7 +703,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
               store_slices<B_TILE>(xb + o + NP * 128, v[u].y);
             }
           } else if (j < n_l) {
-            const double sc = pinv[p] * (1.0 / 16387064.0);
+            const double sc = pinv[p] * 0x1p-24;
             stage_out[j * (NP + 1) + p] = make_double2(v[u].x * sc, v[u].y * sc);
           }
         }
@@ -849,14 +845,14 @@ k_slice_x(const double2* __restrict__ x, int n_r, int n_cols, int cols_pad, int 
     for (int u = 0; u < 4; ++u) {
       const int r = r4 + u;
       const double2 v = r < n_r ? xr[r] : make_double2(0.0, 0.0);
-      int8_t sr[I8_SLICES], si[I8_SLICES];
-      slice4(v.x * sc, sr);
-      slice4(v.y * sc, si);
+      // -Xi is sliced from -x itself: negating a digit -128 would not fit an int8
+      const uint32_t wr = slice_word(v.x * sc * 16777216.0), wi = slice_word(v.y * sc * 16777216.0),
+                     wn = slice_word(-v.y * sc * 16777216.0);
 #pragma unroll
       for (int qq = 0; qq < I8_SLICES; ++qq) {
-        pr[qq] |= (uint32_t)(uint8_t)sr[qq] << (8 * u);
-        pi[qq] |= (uint32_t)(uint8_t)si[qq] << (8 * u);
-        pn[qq] |= (uint32_t)(uint8_t)(int8_t)(-si[qq]) << (8 * u);
+        pr[qq] |= ((wr >> (24 - 8 * qq)) & 0xffu) << (8 * u);
+        pi[qq] |= ((wi >> (24 - 8 * qq)) & 0xffu) << (8 * u);
+        pn[qq] |= ((wn >> (24 - 8 * qq)) & 0xffu) << (8 * u);
       }
     }
 #pragma unroll
