@@ -11,9 +11,14 @@
 //   (|T| < 2^31) and cut into its four balanced base-256 digits, the bytes of T + 0x80808080 each
 //   less 128 (an int8 in [-128, 127]):
 //       v 2^e = a1 + a2 2^-8 + a3 2^-16 + a4 2^-24 (+ at most 2^-25)
-//   A row is resolved to ~2^-31 of its own maximum.  The constant operators are applied every step,
-//   so their representation error is a fixed non-unitarity that compounds: it is what the fourth
-//   slice buys down.
+//   A row is resolved to ~2^-31 of its own maximum.  The constant operators (W_l, the chain
+//   matrices) are applied every step, so a fixed rounding error of theirs compounds linearly over
+//   the pulse (measured: W rounded to nearest alone moves the helium harmonics by 6e-4).  They are
+//   therefore held as several dithered variants, rounded with offsets that cycle through
+//   (j + 1/2) / n_var, and the step counter picks variant (step mod n_var): over n_var steps the
+//   variants average to the exact operator to within 2^-24 / (2 n_var) of the row scale, and what
+//   is left of the rounding is a zero-mean oscillation.  The orbital values are rounded to nearest
+//   afresh at every product, which is already zero-mean.
 //   product: the ten slice pairs (j, m) with j + m <= 3 (0-based; the rest weigh < 2^-32 of the
 //   row maxima and are zero-mean), accumulated exactly in int32 tensor memory, one accumulator per
 //   weight 2^-8(j+m); the epilogue combines the four accumulators exactly (int64 shifts), undoes the
@@ -71,9 +76,27 @@ __device__ __forceinline__ void store_slices(uint8_t* dst, double t3) {
   dst[2 * PLANE] = (uint8_t)(v >> 8);
   dst[3 * PLANE] = (uint8_t)v;
 }
-// the four slices of t (|t| < 126) as int8 values, most significant first
-__device__ __forceinline__ void slice4(double t, int8_t* s) {
-  const uint32_t v = slice_word(t * 16777216.0);
+// Dithered variants of the constant operators: variant v of element (a, b, c) rounds t 2^24 down
+// after adding ((v + h(a, b, c)) mod n_var + 1/2) / n_var.  Over the n_var variants the offsets
+// take every value once, so their mean is t 2^24 to within 1 / (2 n_var); the hash h staggers the
+// cycle from element to element, so that one step's errors are as uncorrelated as rounding to
+// nearest.  n_var is a power of two.
+constexpr int I8_W_VARIANTS = 8;
+constexpr int I8_S_VARIANTS = 16;
+
+__device__ __forceinline__ uint32_t dither_hash(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t h = a * 0x9E3779B1u ^ b * 0x85EBCA77u ^ c * 0xC2B2AE3Du;
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 13;
+  return h;
+}
+__device__ __forceinline__ double dither_offset(int v, int n_var, uint32_t h) {
+  return ((double)((v + (int)(h >> 8)) & (n_var - 1)) + 0.5) / (double)n_var;
+}
+// the four slices of floor(t 2^24 + d) (|t| < 126, 0 < d < 1) as int8 values, most significant first
+__device__ __forceinline__ void slice4_dithered(double t, double d, int8_t* s) {
+  const uint32_t v = ((uint32_t)__double2int_rd(fma(t, 16777216.0, d)) + 0x80808080u) ^ 0x80808080u;
 #pragma unroll
   for (int q = 0; q < I8_SLICES; ++q) s[q] = (int8_t)(uint8_t)(v >> (24 - 8 * q));
 }
@@ -94,7 +117,7 @@ __global__ void k_w_rowmax(const double2* __restrict__ W, int* __restrict__ wexp
 
 // A(i,k) planes, transposed through shared memory (read along i, write along k)
 __global__ void k_slice_w_i8(const double2* __restrict__ W, const int* __restrict__ wexp, int8_t* __restrict__ Wi8,
-                             int n_r, int rows_pad, int k_pad) {
+                             int n_r, int rows_pad, int k_pad, int variant, int n_var) {
   __shared__ double2 t[32][33];
   const int l = blockIdx.z;
   const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
@@ -111,9 +134,10 @@ __global__ void k_slice_w_i8(const double2* __restrict__ W, const int* __restric
     if (i < rows_pad && k < k_pad) {
       const double sc = ldexp(1.0, wexp[(size_t)l * rows_pad + i]);
       const double2 w = t[tx][q];
+      const uint32_t h = dither_hash((uint32_t)l, (uint32_t)i, (uint32_t)k);
       int8_t sr[I8_SLICES], si[I8_SLICES];
-      slice4(w.x * sc, sr);
-      slice4(w.y * sc, si);
+      slice4_dithered(w.x * sc, dither_offset(variant, n_var, h), sr);
+      slice4_dithered(w.y * sc, dither_offset(variant, n_var, h * 0x165667B1u), si);
       const size_t o = (size_t)i * k_pad + k;
 #pragma unroll
       for (int p = 0; p < I8_SLICES; ++p) {
@@ -126,7 +150,7 @@ __global__ void k_slice_w_i8(const double2* __restrict__ W, const int* __restric
 
 // S^T planes of the chain matrices: St[mat][m][slice][j][l] with the row (j) exponents
 __global__ void k_build_st_i8(const double* __restrict__ mats, int8_t* __restrict__ St, int* __restrict__ sexp,
-                              int n_mm, int n_l, int ldS, int rows, int lk) {
+                              int n_mm, int n_m, int n_l, int ldS, int rows, int lk, int variant, int n_var) {
   const int row = blockIdx.x;                 // (mat * n_m + m) * rows + j
   const int mm = row / rows, j = row - mm * rows;
   if (mm >= n_mm) return;
@@ -141,13 +165,14 @@ __global__ void k_build_st_i8(const double* __restrict__ mats, int8_t* __restric
     __syncthreads();
   }
   const int e = row_exponent(red[0]);
-  if (threadIdx.x == 0) sexp[row] = e;
+  if (threadIdx.x == 0 && variant == 0) sexp[row] = e;
   const double sc = ldexp(1.0, e);
   const size_t plane = (size_t)rows * lk;
   for (int l = threadIdx.x; l < lk; l += blockDim.x) {
     const double v = (j < n_l && l < n_l) ? mats[((size_t)mm * n_l + l) * ldS + j] * sc : 0.0;
     int8_t s[I8_SLICES];
-    slice4(v, s);
+    // the hash leaves out m, so that a matrix gets the same variants in any group of runs
+    slice4_dithered(v, dither_offset(variant, n_var, dither_hash((uint32_t)(mm / n_m), (uint32_t)j, (uint32_t)l)), s);
 #pragma unroll
     for (int p = 0; p < I8_SLICES; ++p) St[(size_t)mm * I8_SLICES * plane + p * plane + (size_t)j * lk + l] = s[p];
   }
@@ -210,7 +235,8 @@ template <int BN>
 __global__ void __launch_bounds__(R8_THREADS, 1)
 k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmX,
             const int* __restrict__ wexp, const int* __restrict__ xexp, int n_r, int rows_pad, int n_cols,
-            int cols_pad, int n_l, int n_k_blocks, int stages, double2* __restrict__ Y, unsigned* status) {
+            int cols_pad, int n_l, int n_k_blocks, int stages, const int* __restrict__ step, int n_var,
+            double2* __restrict__ Y, unsigned* status) {
   using T = R8Tile<BN>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ uint64_t full_bar[8], empty_bar[8], accf_bar[2], acce_bar[2], drain_bar;
@@ -249,6 +275,7 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
 
   if (warp == 0) {
     if (lane == 0) {
+      const int var = *step & (n_var - 1);     // this step's variant of W
       int it = 0;
       bool ok = true;
       for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
@@ -262,7 +289,7 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
           }
           uint8_t* st = smem + (size_t)s * T::STAGE;
           mbar_expect_tx(&full_bar[s], T::STAGE);
-          tma_load_4d(st, &tmW, kb * R8_BK, mt * R8_BM, 0, l, &full_bar[s]);
+          tma_load_5d(st, &tmW, kb * R8_BK, mt * R8_BM, 0, l, var, &full_bar[s]);
           tma_load_4d(st + T::A_STAGE, &tmX, kb * R8_BK, nt * BN, 0, l, &full_bar[s]);
         }
       }
@@ -392,6 +419,8 @@ struct Ang8Args {
   const int* sexp;        // S^T row exponents [mat][m][rows]
   int rows;               // m_tiles * 128
   int ld_stage;           // row length of the FP64 staging tiles [NP][ld_stage] (odd when it fits)
+  int n_mats;             // chain matrices per variant
+  int n_var;              // dithered variants of the chain matrices (a power of two)
 };
 
 // Byte offset of (row n, k) of slice plane 0 in the B operand: per 128-wide k atom, the four slice
@@ -474,8 +503,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   const Chain& ch = g.chain[SECOND_HALF ? 1 : 0];
   const int n_ops = ch.n_ops;
   const int acc_cols = 4 * NB;                // per M tile: weights 2^0 .. 2^-24
-  int step = *g.step;
-  if (step >= run.n_t) step = run.n_t - 1;
+  const int step_raw = *g.step;
+  const int step = step_raw < run.n_t ? step_raw : run.n_t - 1;
   const double hdt = 0.5 * g.dt;
   const double* pco = g.coef + ((size_t)CF_P * g.n_m + m) * n_l;
 
@@ -569,7 +598,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       int it = 0;
       bool ok = true;
       for (int o = 0; o < n_ops && ok; ++o) {
-        const int mat = ch.ops[o].mat;
+        const int mat = ch.ops[o].mat + (step_raw & (t.n_var - 1)) * t.n_mats;   // this step's variant
         for (int mt = 0; mt < t.m_tiles && ok; ++mt)
           for (int ka = 0; ka < t.k_atoms && ok; ++ka)
             for (int pa = 0; pa < I8_SLICES; ++pa, ++it) {
@@ -900,12 +929,13 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   q.cols_pad = ((a.n_cols + q.bn - 1) / q.bn) * q.bn;
   q.stages = r8_stages(q.bn);
   // W planes and row exponents
-  const size_t nw = (size_t)n_l * R8_W_PLANES * mg.rows_pad * mg.k_pad;
-  I8_CK(cudaMalloc(&q.W, nw));
+  const size_t nw = (size_t)n_l * R8_W_PLANES * mg.rows_pad * mg.k_pad;    // one variant
+  I8_CK(cudaMalloc(&q.W, nw * I8_W_VARIANTS));
   I8_CK(cudaMalloc(&q.wexp, (size_t)n_l * mg.rows_pad * sizeof(int)));
   k_w_rowmax<<<dim3((mg.rows_pad + 127) / 128, n_l), 128>>>(W_fp64, q.wexp, n_r, mg.rows_pad);
   const dim3 tb(32, 8), tg((mg.rows_pad + 31) / 32, (mg.k_pad + 31) / 32, n_l);
-  k_slice_w_i8<<<tg, tb>>>(W_fp64, q.wexp, q.W, n_r, mg.rows_pad, mg.k_pad);
+  for (int v = 0; v < I8_W_VARIANTS; ++v)
+    k_slice_w_i8<<<tg, tb>>>(W_fp64, q.wexp, q.W + nw * v, n_r, mg.rows_pad, mg.k_pad, v, I8_W_VARIANTS);
   I8_CK(cudaGetLastError());
   // radial B operand planes
   const size_t nx = (size_t)n_l * R8_X_PLANES * q.cols_pad * mg.k_pad;
@@ -919,12 +949,13 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
     return GGB_ERR_CUDA;
   }
   {
-    cuuint64_t dims[4] = {(cuuint64_t)mg.k_pad, (cuuint64_t)mg.rows_pad, R8_W_PLANES, (cuuint64_t)n_l};
-    cuuint64_t strides[3] = {(cuuint64_t)mg.k_pad, (cuuint64_t)mg.rows_pad * mg.k_pad,
-                             (cuuint64_t)R8_W_PLANES * mg.rows_pad * mg.k_pad};
-    cuuint32_t box[4] = {R8_BK, R8_BM, R8_W_PLANES, 1};
-    cuuint32_t es[4] = {1, 1, 1, 1};
-    if (enc(&q.tmW, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, q.W, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    cuuint64_t dims[5] = {(cuuint64_t)mg.k_pad, (cuuint64_t)mg.rows_pad, R8_W_PLANES, (cuuint64_t)n_l,
+                          (cuuint64_t)I8_W_VARIANTS};
+    cuuint64_t strides[4] = {(cuuint64_t)mg.k_pad, (cuuint64_t)mg.rows_pad * mg.k_pad,
+                             (cuuint64_t)R8_W_PLANES * mg.rows_pad * mg.k_pad, (cuuint64_t)nw};
+    cuuint32_t box[5] = {R8_BK, R8_BM, R8_W_PLANES, 1, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    if (enc(&q.tmW, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, q.W, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
         CUDA_SUCCESS) {
       err = "tensor map (int8 W) failed";
@@ -975,12 +1006,18 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   const int rows = 128 * q.a_m_tiles, lk = A8_KATOM * q.a_k_atoms;
   q.a_rows = rows;
   const int n_mm = n_mats * a.n_m;
-  I8_CK(cudaMalloc(&q.St, (size_t)n_mm * I8_SLICES * rows * lk));
+  const size_t nst = (size_t)n_mm * I8_SLICES * rows * lk;    // one variant
+  q.n_mats = n_mats;
+  I8_CK(cudaMalloc(&q.St, nst * I8_S_VARIANTS));
   I8_CK(cudaMalloc(&q.sexp, (size_t)n_mm * rows * sizeof(int)));
-  k_build_st_i8<<<n_mm * rows, 256>>>(a.mats, q.St, q.sexp, n_mm, n_l, a.ldS, rows, lk);
+  for (int v = 0; v < I8_S_VARIANTS; ++v)
+    k_build_st_i8<<<n_mm * rows, 256>>>(a.mats, q.St + nst * v, q.sexp, n_mm, a.n_m, n_l, a.ldS, rows, lk, v,
+                                        I8_S_VARIANTS);
   I8_CK(cudaGetLastError());
   {
-    cuuint64_t dims[5] = {(cuuint64_t)lk, (cuuint64_t)rows, I8_SLICES, (cuuint64_t)a.n_m, (cuuint64_t)n_mats};
+    // the variants follow one another along the matrix index: matrix mat of variant v is mat + v n_mats
+    cuuint64_t dims[5] = {(cuuint64_t)lk, (cuuint64_t)rows, I8_SLICES, (cuuint64_t)a.n_m,
+                          (cuuint64_t)n_mats * I8_S_VARIANTS};
     cuuint64_t strides[4] = {(cuuint64_t)lk, (cuuint64_t)rows * lk, (cuuint64_t)I8_SLICES * rows * lk,
                              (cuuint64_t)a.n_m * I8_SLICES * rows * lk};
     cuuint32_t box[5] = {A8_KATOM, 128, 1, 1, 1};
@@ -1016,9 +1053,9 @@ void int8_radial(MixedGroup& mg, const GroupArgs& a, cudaStream_t s) {
   const dim3 g(tiles < q.ctas ? tiles : q.ctas);
   const int nkb = mg.k_pad / R8_BK;
   switch (q.bn) {
-    case 16: k_radial_i8<16><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, mg.Yd, a.status); break;
-    case 32: k_radial_i8<32><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, mg.Yd, a.status); break;
-    default: k_radial_i8<64><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, mg.Yd, a.status); break;
+    case 16: k_radial_i8<16><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, a.step, I8_W_VARIANTS, mg.Yd, a.status); break;
+    case 32: k_radial_i8<32><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, a.step, I8_W_VARIANTS, mg.Yd, a.status); break;
+    default: k_radial_i8<64><<<g, R8_THREADS, q.smem, s>>>(q.tmW, q.tmX, q.wexp, q.xexp, a.n_r, mg.rows_pad, a.n_cols, q.cols_pad, a.n_l, nkb, q.stages, a.step, I8_W_VARIANTS, mg.Yd, a.status); break;
   }
 }
 
@@ -1032,6 +1069,8 @@ void int8_angular(MixedGroup& mg, const GroupArgs& a, int half, const double2* x
   t.sexp = q.sexp;
   t.rows = q.a_rows;
   t.ld_stage = q.a_ld;
+  t.n_mats = q.n_mats;
+  t.n_var = I8_S_VARIANTS;
   const dim3 grid(a.n_cols * ((a.n_r + q.np - 1) / q.np));
   if (q.np == 32) {
     if (half == 0) k_angular_i8<32, false><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout);

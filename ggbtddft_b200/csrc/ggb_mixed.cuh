@@ -20,11 +20,12 @@ constexpr unsigned ST_TC_TIMEOUT = 8u;   // a bounded wait in a tensor-core kern
 // Integer-split form (ggb_int8.cu): int8 slice planes of W, of the chain matrices and of the radial
 // B operand, with per-row power-of-two exponents of the constant operators.
 struct I8Group {
-  int8_t* W = nullptr;       // [N_l][8][rows_pad][k_pad]: Wr slices 1-4, Wi slices 1-4; A(i,k) = W[l][k][i] 2^e(l,i)
+  int8_t* W = nullptr;       // [variant][N_l][8][rows_pad][k_pad]: Wr slices 1-4, Wi slices 1-4; A(i,k) = W[l][k][i] 2^e(l,i)
   int* wexp = nullptr;       // [N_l][rows_pad]
   int8_t* X = nullptr;       // [N_l][12][cols_pad][k_pad]: Xr, Xi, -Xi slices 1-4 of x 2^xexp(l, col)
   int* xexp = nullptr;       // [N_l][cols_pad]
-  int8_t* St = nullptr;      // [mat][m][4][rows][lk]: S^T slices, rows scaled by 2^sexp
+  int8_t* St = nullptr;      // [variant][mat][m][4][rows][lk]: S^T slices, rows scaled by 2^sexp
+  int n_mats = 0;            // chain matrices per variant
   int* sexp = nullptr;       // [mat][m][rows]
   CUtensorMap tmW, tmX, tmS;
   int bn = 16, cols_pad = 0, stages = 2, ctas = 0;
