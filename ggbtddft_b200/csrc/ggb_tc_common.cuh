@@ -42,6 +42,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 // Wait for the phase of `parity`.  Gives up (returns false, raises the abort flag) after the time
 // limit, or as soon as another role of the CTA has aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try(b, parity)) return true;   // the common case reads no timer
   const uint64_t t0 = gtimer();
   while (!mbar_try(b, parity)) {
     if (*abort_flag) return false;
