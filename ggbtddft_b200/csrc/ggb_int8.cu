@@ -621,35 +621,37 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       // accumulator of weight 2^-8(pa + pb)
       const uint32_t idesc[I8_SLICES] = {idesc_i8(128, 4 * NB), idesc_i8(128, 3 * NB), idesc_i8(128, 2 * NB),
                                           idesc_i8(128, NB)};
-      const uint32_t sxb = smem_u32(xb);
-      int it = 0;
+      // The loads come four per (M tile, k atom), one per slice plane pa, into a ring of four
+      // stages, so stage pa always holds plane pa and the ring turns once per (tile, atom).  The
+      // descriptors of stage pa and k step kk are those of stage 0 (or of the B operand's atom) plus
+      // the byte offset / 16 in the start-address field, which keeps this thread's loop short: it
+      // shares its SM sub-partition with busy epilogue warps, and its issue rate paces the products.
+      const uint64_t adesc = sdesc_kmajor(smem_u32(sst), 128, 2);
+      const uint64_t bdesc = sdesc_kmajor(smem_u32(xb), 128, 2);
+      int round = 0;
       for (int o = 0; o < n_ops; ++o) {
         if (o > 0 && !mbar_wait(&xb_bar, (o - 1) & 1, abort_p)) break;
         tc_fence_after();
         bool ok = true;
         for (int mt = 0; mt < t.m_tiles && ok; ++mt) {
           const uint32_t d0 = tmem + acc_cols * mt;
-          for (int ka = 0; ka < t.k_atoms && ok; ++ka)
-            for (int pa = 0; pa < I8_SLICES; ++pa, ++it) {
-              const int s = it % t.stages;
-              if (!mbar_wait(&full_bar[s], (it / t.stages) & 1, abort_p)) {
+          for (int ka = 0; ka < t.k_atoms && ok; ++ka, ++round) {
+            const uint64_t bk = bdesc + (uint64_t)((ka * I8_SLICES * B_TILE) >> 4);
+            const int nk = min(A8_KATOM / 32, t.k_steps - ka * (A8_KATOM / 32));
+#pragma unroll
+            for (int pa = 0; pa < I8_SLICES; ++pa) {
+              if (!mbar_wait(&full_bar[pa], round & 1, abort_p)) {
                 ok = false;
                 break;
               }
               tc_fence_after();
-              const uint32_t sa = smem_u32(sst + (size_t)s * A8_A_TILE);
+              const uint64_t ak = adesc + (uint64_t)((pa * A8_A_TILE) >> 4);
 #pragma unroll
-              for (int kk = 0; kk < A8_KATOM / 32; ++kk) {
-                const int kstep = ka * (A8_KATOM / 32) + kk;
-                if (kstep >= t.k_steps) break;
-                const uint32_t ko = kk * 32;
-                const uint64_t a = sdesc_kmajor(sa + ko, 128, 2);
-                const uint64_t b = sdesc_kmajor(sxb + ka * I8_SLICES * B_TILE + ko, 128, 2);
-                const uint32_t first = (kstep == 0 && pa == 0) ? 0u : 1u;
-                tc_mma_i8(d0 + pa * NB, a, b, idesc[pa], first);
-              }
-              tc_commit(&empty_bar[s]);
+              for (int kk = 0; kk < A8_KATOM / 32; ++kk)
+                if (kk < nk) tc_mma_i8(d0 + pa * NB, ak + 2 * kk, bk + 2 * kk, idesc[pa], (ka | kk | pa) ? 1u : 0u);
+              tc_commit(&empty_bar[pa]);
             }
+          }
         }
         // one commit for all M tiles: every tile's products read the whole operand, which the
         // epilogue overwrites with the next product's
@@ -985,7 +987,7 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
   // two CTAs per SM: 256 TMEM columns each (NP points x {Re, Im} x 4 accumulators x M tiles) and
   // at most ~110 KB of shared memory each
   q.np = q.a_m_tiles == 1 ? 32 : 16;     // the kernel takes k_atoms = m_tiles = (NP == 32 ? 1 : 2)
-  q.a_stages = 4;
+  q.a_stages = I8_SLICES;   // the MMA issue loop relies on stage = slice plane
   q.a_smem = q.np == 32 ? a8_smem<32>(q.a_k_atoms, q.a_stages) : a8_smem<16>(q.a_k_atoms, q.a_stages);
   // FP64 staging: the input tile [NP][ld] in the stage buffers (an odd ld when it fits), the last
   // product [N_l][NP + 1] over the operand planes and stage buffers
