@@ -300,7 +300,10 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
     if (lane == 0) {
       const uint32_t idesc[I8_SLICES] = {idesc_i8(R8_BM, 4 * BN), idesc_i8(R8_BM, 3 * BN), idesc_i8(R8_BM, 2 * BN),
                                           idesc_i8(R8_BM, BN)};
-      int it = 0, local = 0;
+      // descriptors: those of stage 0 plus the byte offset / 16 in the start-address field (this
+      // thread's issue rate paces the products)
+      const uint64_t desc0 = sdesc_kmajor(smem_u32(smem), 32, 6);
+      int local = 0, s = 0, ph = 0;
       for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++local) {
         const int buf = (T::NBUF == 2) ? (local & 1) : 0;
         const int use = (T::NBUF == 2) ? (local >> 1) : local;
@@ -308,25 +311,23 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
         tc_fence_after();
         const uint32_t d0 = tmem + buf * T::ACC_COLS;
         bool ok = true;
-        for (int kb = 0; kb < n_k_blocks; ++kb, ++it) {
-          const int s = it % stages;
-          if (!mbar_wait(&full_bar[s], (it / stages) & 1, abort_p)) {
+        for (int kb = 0; kb < n_k_blocks; ++kb) {
+          if (!mbar_wait(&full_bar[s], ph, abort_p)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t sa = smem_u32(smem + (size_t)s * T::STAGE);
-          const uint32_t sb = sa + T::A_STAGE;
+          const uint64_t da = desc0 + (uint64_t)(((uint32_t)s * T::STAGE) >> 4);
           // one 32-wide k block: for each W slice j, one MMA per real product covers the x slices
           // m = 0 .. 3 - j at once (the x planes of each kind are contiguous rows), N = (4 - j) BN,
           // written from accumulator group j on, so that column group m lands on weight 2^-8(j+m)
-          const uint64_t xr = sdesc_kmajor(sb, 32, 6);
-          const uint64_t xi = sdesc_kmajor(sb + I8_SLICES * T::B_PLANE, 32, 6);
-          const uint64_t xn = sdesc_kmajor(sb + 2 * I8_SLICES * T::B_PLANE, 32, 6);
+          const uint64_t xr = da + (T::A_STAGE >> 4);
+          const uint64_t xi = xr + ((I8_SLICES * T::B_PLANE) >> 4);
+          const uint64_t xn = xr + ((2 * I8_SLICES * T::B_PLANE) >> 4);
 #pragma unroll
           for (int j = 0; j < I8_SLICES; ++j) {
-            const uint64_t wr = sdesc_kmajor(sa + j * T::A_PLANE, 32, 6);
-            const uint64_t wi = sdesc_kmajor(sa + (I8_SLICES + j) * T::A_PLANE, 32, 6);
+            const uint64_t wr = da + ((j * T::A_PLANE) >> 4);
+            const uint64_t wi = da + (((I8_SLICES + j) * T::A_PLANE) >> 4);
             const uint32_t dre = d0 + j * BN, dim = d0 + (4 + j) * BN;
             const uint32_t first = (kb == 0 && j == 0) ? 0u : 1u;
             tc_mma_i8(dre, wr, xr, idesc[j], first);
@@ -335,6 +336,10 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
             tc_mma_i8(dim, wi, xr, idesc[j], 1u);
           }
           tc_commit(&empty_bar[s]);
+          if (++s == stages) {
+            s = 0;
+            ph ^= 1;
+          }
         }
         tc_commit(&accf_bar[buf]);
         if (!ok) break;
@@ -599,17 +604,20 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       bool ok = true;
       for (int o = 0; o < n_ops && ok; ++o) {
         const int mat = ch.ops[o].mat + (step_raw & (t.n_var - 1)) * t.n_mats;   // this step's variant
+        // stage pa takes slice plane pa; the ring turns once per (tile, atom)
         for (int mt = 0; mt < t.m_tiles && ok; ++mt)
-          for (int ka = 0; ka < t.k_atoms && ok; ++ka)
+          for (int ka = 0; ka < t.k_atoms && ok; ++ka) {
+            const int round = it / I8_SLICES;
+#pragma unroll
             for (int pa = 0; pa < I8_SLICES; ++pa, ++it) {
-              const int s = it % t.stages;
-              if (it >= t.stages && !mbar_wait(&empty_bar[s], ((it / t.stages) & 1) ^ 1, abort_p)) {
+              if (round > 0 && !mbar_wait(&empty_bar[pa], (round & 1) ^ 1, abort_p)) {
                 ok = false;
                 break;
               }
-              mbar_expect_tx(&full_bar[s], A8_A_TILE);
-              tma_load_5d(sst + (size_t)s * A8_A_TILE, &tmS, ka * A8_KATOM, mt * 128, pa, m, mat, &full_bar[s]);
+              mbar_expect_tx(&full_bar[pa], A8_A_TILE);
+              tma_load_5d(sst + pa * A8_A_TILE, &tmS, ka * A8_KATOM, mt * 128, pa, m, mat, &full_bar[pa]);
             }
+          }
       }
       if (!ok)
         for (int q = (it > t.stages ? it - t.stages : 0); q < it; ++q) mbar_drain(&full_bar[q % t.stages], (q / t.stages) & 1);
