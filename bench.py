@@ -64,6 +64,16 @@ def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8"):
                                           "9 orbitals each), 800 nm 10-cycle sin^2 at 0.8-1.2 x 1.4e14 W/cm^2; "
                                           "first steps of the pulse", runs=16, n_r=600, l_max=96, n_orb=9,
                                  precision=split)
+    if name == "ar16-n400-l160":
+        # the angular size of the largest rung of the ensemble (N_l = 161: two M tiles of channels)
+        # on a shorter radial grid, small enough for a full ncu capture
+        base = P.baseline_run("Ar", 400, 200.0, 160, 0.02, P.LaserSpec(1.4e14, 800.0, 10.0, 0.0), 40.0,
+                              n_steps=n_t, device=device)
+        runs = [base.with_field(base.E * s) for s in np.linspace(0.8, 1.2, 16)]
+        return runs, split, dict(workload="16 argon LDA runs on one grid (N_r=400, r_max=200, l_max=160, dt=0.02; "
+                                          "9 orbitals each), 800 nm 10-cycle sin^2 at 0.8-1.2 x 1.4e14 W/cm^2; "
+                                          "first steps of the pulse", runs=16, n_r=400, l_max=160, n_orb=9,
+                                 precision=split)
     if name == "ar-split":
         run = P.config_argon(n_steps=n_t, device=device)
         return [run], split, dict(workload="Ar LDA, 9 orbitals, N_r=600, r_max=300, l_max=96, dt=0.02",
@@ -160,6 +170,34 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# DRAM traffic per algorithmic byte, dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture
+# (--set full, cold caches) over the launch's algorithmic bytes, for the split_int8 kernels of the
+# committed profiling workloads: ar16-n600 (N_l = 97, the one-M-tile kernel, and the radial product)
+# and ar16-n400-l160 (N_l = 161, the two-M-tile kernel).  The ensemble is too large to capture whole;
+# its traffic is estimated group by group from these ratios (orbital traffic grows in proportion to
+# N_r N_l columns; W in proportion to N_r^2 N_l).
+MEASURED_TRAFFIC_RATIO = {
+    ("split_int8", "radial", 1): 554.63 / 514.02, ("split_int8", "radial", 2): 554.63 / 514.02,
+    ("split_int8", "angular_first", 1): 212.18 / 268.19, ("split_int8", "angular_second", 1): 241.05 / 268.19,
+    ("split_int8", "angular_first", 2): 243.06 / 296.76, ("split_int8", "angular_second", 2): 291.07 / 296.76,
+}
+TRAFFIC_SOURCE = ("per group: algorithmic bytes x (DRAM bytes / algorithmic bytes) of an ncu capture of the same "
+                  "kernel on ar16-n600 (one M tile, radial) or ar16-n400-l160 (two M tiles)")
+
+
+def measured_traffic(runs, groups, precision, phase):
+    """Estimated DRAM bytes of one launch of `phase` (all groups), or None without a capture."""
+    total = 0.0
+    for members in groups:
+        sub = phase_traffic(runs, [members], precision)[phase]["bytes"]
+        m_tiles = 1 if runs[members[0]].n_l <= 128 else 2
+        ratio = MEASURED_TRAFFIC_RATIO.get((precision, phase, m_tiles))
+        if ratio is None:
+            return None
+        total += sub * ratio
+    return total
 
 
 def phase_traffic(runs, groups, precision):
@@ -266,33 +304,39 @@ def run_ours(args, rank, world, dist):
         tp2.close()
         e2e_value = world * units_per_step * args.steps / e2e_s
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel (the phase with the longest device time per step): the HBM
+    # bound (algorithmic bytes) and, for the split forms, the tensor bound (executed split products)
+    # are both evaluated and the larger fraction is reported; every phase's figures stay in `kernels`
     tf = phase_traffic(runs, tp.groups, precision)
     dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
     tensor_peak = read_peaks()[1] * TENSOR_PEAK_FACTOR[precision] if precision != "fp64" else None
+    sp = SPLIT_PRODUCTS.get(precision, 1)
     kernels = {}
     for k in ("radial", "angular_first", "angular_second"):
         sec = phase_ms[k] / 1e3
         kernels[k] = dict(ms=round(phase_ms[k], 5), algorithmic_bytes=int(tf[k]["bytes"]),
-                          gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3))
+                          gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3),
+                          hbm_frac=round(tf[k]["bytes"] / sec / 1e9 / hbm_peak, 4))
+        if tensor_peak:
+            kernels[k]["tensor_frac_executed"] = round(sp * tf[k]["flops"] / sec / 1e12 / tensor_peak, 4)
     kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
-    rad = kernels["radial"]
-    name = {"fp64": "k_radial_fp64", "split_bf16": "k_radial_tc_persistent (tcgen05 kind::f16, split BF16)",
-            "split_int8": "k_radial_i8 (tcgen05 kind::i8, int8 slices, int32 accumulation)"}[precision]
-    roofline = dict(bound="hbm", kernel=f"radial propagator ({name})", achieved=rad["gbs"], peak=hbm_peak,
-                    unit="GB/s", frac=round(rad["gbs"] / hbm_peak, 4), traffic=None,
+    names = {"radial": {"fp64": "k_radial_fp64", "split_bf16": "k_radial_tc_persistent (tcgen05 kind::f16)",
+                        "split_int8": "k_radial_i8 (tcgen05 kind::i8, int8 slices, int32 accumulation)"},
+             "angular": {"fp64": "k_angular_fp64", "split_bf16": "k_angular_tc (tcgen05 kind::f16)",
+                         "split_int8": "k_angular_i8 (tcgen05 kind::i8 chain, FP64 phases)"}}
+    d = kernels[dom]
+    kname = names["radial" if dom == "radial" else "angular"][precision]
+    est = measured_traffic(runs, tp.groups, precision, dom)
+    roofline = dict(bound="hbm", kernel=f"{dom} ({kname})", achieved=d["gbs"], peak=hbm_peak, unit="GB/s",
+                    frac=d["hbm_frac"], traffic=None if est is None else int(est),
+                    traffic_source=None if est is None else TRAFFIC_SOURCE,
                     peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom, kernels=kernels)
-    if tensor_peak:
-        # every real product runs as several split products on the tensor cores
-        sp = SPLIT_PRODUCTS[precision]
-        roofline["tensor_frac_alg"] = round(rad["tflops"] / tensor_peak, 4)
-        roofline["tensor_frac_executed"] = round(sp * rad["tflops"] / tensor_peak, 4)
-        if roofline["tensor_frac_executed"] > roofline["frac"]:
-            pk = f"{peak_kind} bf16_tflops" + (" x2 (int8)" if precision == "split_int8" else "")
-            roofline.update(bound="tensor", achieved=round(sp * rad["tflops"], 3), peak=round(tensor_peak, 1),
-                            unit="TFLOP/s (executed split products)" if precision == "split_bf16"
-                            else "TOP/s (executed int8 slice products)",
-                            frac=roofline["tensor_frac_executed"], peak_kind=pk)
+    if tensor_peak and d["tensor_frac_executed"] > d["hbm_frac"]:
+        pk = f"{peak_kind} bf16_tflops" + (" x2 (int8)" if precision == "split_int8" else "")
+        roofline.update(bound="tensor", achieved=round(sp * d["tflops"], 3), peak=round(tensor_peak, 1),
+                        unit="TFLOP/s (executed split products)" if precision == "split_bf16"
+                        else "TOP/s (executed int8 slice products)",
+                        frac=d["tensor_frac_executed"], peak_kind=pk)
     # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU
     fp64_inst = None
     if args.compare_fp64 and (len(runs) > 1 or precision != "fp64"):
