@@ -88,7 +88,9 @@ k_angular_tc(const __grid_constant__ CUtensorMap tmS, GroupArgs g, AngTcArgs t, 
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   __shared__ float pbase[5][AT_NP];     // per point: r, (r E + v1 or r E) dt/2, v2 dt/2, v3 dt/2, S base dt/2
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  // aligned by an offset from the __shared__ array itself, so that the compiler keeps the shared
+  // address space (shared loads and stores, not generic ones) for every access through it
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* xb = smem;                                            // 2 planes x k_atoms x 16 KB
   uint8_t* sst = smem + (size_t)2 * t.k_atoms * AT_B_TILE;       // stages x 32 KB (later: FP32 staging)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -242,7 +242,9 @@ k_radial_i8(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
   __shared__ uint64_t full_bar[8], empty_bar[8], accf_bar[2], acce_bar[2], drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  // aligned by an offset from the __shared__ array itself, so that the compiler keeps the shared
+  // address space (shared loads and stores, not generic ones) for every access through it
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m_tiles = (n_r + R8_BM - 1) / R8_BM, n_tiles = (n_cols + BN - 1) / BN;
   const int total = m_tiles * n_tiles * n_l;
@@ -495,7 +497,9 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   __shared__ double pbase[5][NP];
   __shared__ double pnorm2[NP];
   __shared__ double pscale3[NP], pinv[NP];    // 2^e(p) 2^24 and 2^-e(p) of each point's B rows
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  // aligned by an offset from the __shared__ array itself, so that the compiler keeps the shared
+  // address space (shared loads and stores, not generic ones) for every access through it
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* xb = smem;                                              // 4 planes x k_atoms x B_TILE
   uint8_t* sst = smem + (size_t)I8_SLICES * XPLANE;                 // stages x 16 KB
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -323,7 +323,9 @@ k_radial_tc(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUt
   __shared__ uint64_t full_bar[8], empty_bar[8], acc_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  // aligned by an offset from the __shared__ array itself, so that the compiler keeps the shared
+  // address space (shared loads and stores, not generic ones) for every access through it
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * RT_BM;
   const int c0 = blockIdx.y * BN;
@@ -452,7 +454,9 @@ k_radial_tc_persistent(const __grid_constant__ CUtensorMap tmW, const __grid_con
   __shared__ uint64_t full_bar[8], empty_bar[8], accf_bar[2], acce_bar[2], drain_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  // aligned by an offset from the __shared__ array itself, so that the compiler keeps the shared
+  // address space (shared loads and stores, not generic ones) for every access through it
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m_tiles = (n_r + RT_BM - 1) / RT_BM, n_tiles = (n_cols + BN - 1) / BN;
   const int total = m_tiles * n_tiles * n_l;
