@@ -232,6 +232,21 @@ def phase_traffic(runs, groups, precision):
 # arms
 # ---------------------------------------------------------------------------------------------
 
+def max_over_ranks(ms: float, dist: bool, device: str = "cuda") -> float:
+    """The slowest rank's timed milliseconds; every rank calls this once, at the same point."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_step: int, steps: int, ms_max: float) -> float:
+    """Orbital-steps/s of the whole job: every replica's units over the slowest replica's time."""
+    return world * units_per_step * steps / (ms_max / 1e3)
+
+
 def run_ours(args, rank, world, dist):
     import torch
     from ggbtddft_b200.engine import TimePropagation
@@ -257,16 +272,14 @@ def run_ours(args, rank, world, dist):
         tp.step(args.steps, h)
         e1.record(stream)
         torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
     ms = e0.elapsed_time(e1)
     st, msg = tp.status()
     if st != 0:
         raise SystemExit(f"device status {st}: {msg}")
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * units_per_step * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist)
+    value = whole_job_rate(world, units_per_step, args.steps, ms_max)
 
     # per-kernel durations (each phase launched alone, CUDA events on the launching stream)
     reps = 20
