@@ -8,7 +8,7 @@ reference's ``output/`` tree and ``case.json``) and writes ``tests/golden/ref_<c
     E        float64 [N_t]                  the E%03d.bin file the run used (h_writeField)
     case     JSON text: the input-generator arguments (problems.reference_like) of the case
 
-Usage:  python tests/golden/make_ref_fixtures.py gpurun_out/ref
+Usage:  python tests/golden/make_ref_fixtures.py <dir>   (the directory oracle/run_ref.sh wrote)
 """
 import json
 import os
