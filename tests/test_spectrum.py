@@ -34,3 +34,22 @@ def test_reference_l_selection():
     tot = S.total_dipole(d, l_active=[0, 1], m_active=[0, 1], occ=[2, 4])
     # kso 0: l = 1..5 (l = 0 excluded) -> 5 terms x 2; kso 1: l_kso == m_kso -> from 1, l = 2..5 -> 4 terms x 4
     assert np.allclose(tot, 5 * 2 + 4 * 4)
+
+
+def test_batched_spectrum_matches_the_single_series_restatement():
+    """The batched (torch, device-agnostic) spectrum and harmonic bands equal hhg_spectrum and
+    harmonic_intensities run one series at a time (here on the CPU; "cuda" runs the same code)."""
+    rng = np.random.default_rng(3)
+    n_t, dt = 1500, 0.05
+    t = np.arange(n_t) * dt
+    w0s = [0.057, 0.045, 0.035]
+    d = np.stack([np.sin(w0 * t) * np.sin(np.pi * t / t[-1]) ** 2 + 1e-3 * np.sin(7 * w0 * t)
+                  + 1e-6 * rng.standard_normal(n_t) for w0 in w0s])
+    w, spec = S.hhg_spectra_batched(d, dt, device="cpu")
+    inten = S.harmonic_intensities_batched(w, spec, w0s, 15)
+    for b, w0 in enumerate(w0s):
+        w1, s1 = S.hhg_spectrum(d[b], dt)
+        np.testing.assert_allclose(w, w1, rtol=0, atol=0)
+        np.testing.assert_allclose(spec[b].numpy(), s1, rtol=1e-9, atol=1e-12 * s1.max())
+        np.testing.assert_allclose(inten[b], S.harmonic_intensities(w1, s1, w0, 15), rtol=1e-9,
+                                   atol=1e-12 * s1.max())
