@@ -1,0 +1,35 @@
+"""The bench's algorithmic bytes/flops per phase and its DRAM-traffic estimate (CPU)."""
+from types import SimpleNamespace
+
+import pytest
+
+import bench
+
+
+def _run(n_r, l_max, n_orb=9, hartree=True):
+    return SimpleNamespace(n_r=n_r, n_l=l_max + 1, n_orb=n_orb, use_hartree=hartree, target_id=1, n_har=4)
+
+
+def test_phase_bytes_and_flops_of_one_int8_group():
+    runs = [_run(600, 96) for _ in range(16)]
+    tf = bench.phase_traffic(runs, [list(range(16))], "split_int8")
+    elems = 600 * 97 * 144
+    # W as eight int8 planes, x as 12 B of slices in, complex128 out
+    assert tf["radial"]["bytes"] == 8 * 600 * 600 * 97 + (12 + 16) * elems
+    assert tf["radial"]["flops"] == 8.0 * 600 * 600 * 97 * 144
+    # complex128 in and out; five chain products with all four couplings
+    assert tf["angular_first"]["bytes"] == 2 * 16 * elems
+    assert tf["angular_second"]["flops"] == 5 * 4.0 * 97 * 97 * 600 * 144
+
+
+def test_traffic_estimate_uses_the_ratio_of_each_groups_kernel():
+    runs = [_run(600, 96), _run(600, 96), _run(900, 144)]
+    groups = [[0, 1], [2]]
+    est = bench.measured_traffic(runs, groups, "split_int8", "angular_second")
+    one = bench.phase_traffic(runs, [[0, 1]], "split_int8")["angular_second"]["bytes"]
+    two = bench.phase_traffic(runs, [[2]], "split_int8")["angular_second"]["bytes"]
+    r1 = bench.MEASURED_TRAFFIC_RATIO[("split_int8", "angular_second", 1)]
+    r2 = bench.MEASURED_TRAFFIC_RATIO[("split_int8", "angular_second", 2)]
+    assert est == pytest.approx(one * r1 + two * r2)
+    # no capture for this form: no estimate
+    assert bench.measured_traffic(runs, groups, "fp64", "angular_second") is None
