@@ -7,7 +7,8 @@
 //
 // Representation (Ozaki-style split, base 256):
 //   every operand row (a row of W_l, of a chain matrix S^T, of orbital values) is scaled by a power
-//   of two 2^e that puts its largest |value| in [63, 126), rounded once to T = rint(v 2^e 2^24)
+//   of two 2^e that puts its largest |value| in [63, 126), rounded once to an integer T ~ v 2^e 2^24
+//   (to nearest for orbital values; dithered for the constant operators, below)
 //   (|T| < 2^31) and cut into its four balanced base-256 digits, the bytes of T + 0x80808080 each
 //   less 128 (an int8 in [-128, 127]):
 //       v 2^e = a1 + a2 2^-8 + a3 2^-16 + a4 2^-24 (+ at most 2^-25)
@@ -25,8 +26,8 @@
 //   two row scales exactly and rounds once to FP64.  The orbitals stay complex128 between products.
 //   int32 range: |a b| <= 2^14, at most 8 products per k and accumulator, K <= 8192: <= 2^30.
 //
-//  k_slice_w_i8      W[l][k][i] -> A(i,k) planes [l][8][rows][k] (Wr a1..a4, Wi a1..a4) + exponents
-//  k_build_st_i8     chain matrices -> S^T planes [mat][m][4][rows][lk] + exponents
+//  k_slice_w_i8      W[l][k][i] -> A(i,k) planes [variant][l][8][rows][k] (Wr a1..a4, Wi a1..a4) + exponents
+//  k_build_st_i8     chain matrices -> S^T planes [variant n_mats + mat][m][4][rows][lk] + exponents
 //  k_slice_x         orbitals (complex128) -> radial B operand planes (Xr, Xi, -Xi) + exponents
 //  k_radial_i8       persistent radial product, kind::i8, 32-byte swizzle, 16 MMAs per 32-wide k block
 //                    (each covers all x slices m of one W slice j):
