@@ -153,19 +153,18 @@ def _coupling(x, prob: OracleProblem, name: str, eta_r: Optional[np.ndarray]):
     """
     V = prob.V[name]
     D = prob.D[name]
-    out = np.empty_like(x)
-    for k in range(prob.n_kso):
-        m = int(prob.m[k])
-        Vm = V[m]
-        xr = np.zeros((prob.n_l, prob.n_r), dtype=np.complex128)
-        xr[m:] = Vm[m:, m:].T @ x[m:, k, :]
+    out = np.zeros_like(x)
+    # the orbitals that share m share V, D and the phase: one product for all of them
+    for m in sorted(set(int(v) for v in prob.m)):
+        ks = [k for k in range(prob.n_kso) if int(prob.m[k]) == m]
+        Vm = V[m][m:, m:]
+        xm = x[m:][:, ks, :].reshape(prob.n_l - m, len(ks) * prob.n_r)
+        xr = (Vm.T @ xm).reshape(prob.n_l - m, len(ks), prob.n_r)
         if eta_r is not None:
-            eta = eta_r[None, :] * ((0.5 * prob.dt) * D[m, m:])[:, None]
-            xr[m:] = (np.cos(eta) * xr[m:].real + np.sin(eta) * xr[m:].imag) + 1j * (
-                np.cos(eta) * xr[m:].imag - np.sin(eta) * xr[m:].real)
-        y = np.zeros((prob.n_l, prob.n_r), dtype=np.complex128)
-        y[m:] = Vm[m:, m:] @ xr[m:]
-        out[:, k, :] = y
+            eta = (eta_r[None, :] * ((0.5 * prob.dt) * D[m, m:])[:, None])[:, None, :]
+            xr = (np.cos(eta) * xr.real + np.sin(eta) * xr.imag) + 1j * (np.cos(eta) * xr.imag - np.sin(eta) * xr.real)
+        y = (Vm @ xr.reshape(prob.n_l - m, len(ks) * prob.n_r)).reshape(prob.n_l - m, len(ks), prob.n_r)
+        out[m:, ks, :] = y
     return out
 
 
@@ -365,8 +364,9 @@ class OracleState:
         x = cD(x)
         x = cP(x)
         x = cS(x)
-        # h_propagationH0: cublasZgemmBatched, A column-major => x_l <- W_l^T x_l (W is complex-symmetric)
-        x = np.einsum("lba,lkb->lka", p.W, x, optimize=True)
+        # h_propagationH0: cublasZgemmBatched, A column-major => x_l <- W_l^T x_l (W is complex-symmetric):
+        # out[l][k][a] = sum_b W[l][b][a] x[l][k][b], one BLAS product per l
+        x = np.matmul(x, p.W)
         x = cS(x)
         x = cP(x)
         x = cD(x)
