@@ -599,6 +599,19 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream) {
   return GGB_OK;
 }
 
+int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages) {
+  if (!ctx) return GGB_ERR_ARG;
+  if (group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, GGB_ERR_ARG, "group %d out of range", group);
+  if (ctx->prepared) return fail(ctx, GGB_ERR_STATE, "ggb_set_tuning after the first ggb_step");
+  if (radial_bn != 0 && radial_bn != 16 && radial_bn != 32 && radial_bn != 64)
+    return fail(ctx, GGB_ERR_ARG, "radial_bn %d is not 0, 16, 32 or 64", radial_bn);
+  if (radial_stages != 0 && (radial_stages < 2 || radial_stages > 8))
+    return fail(ctx, GGB_ERR_ARG, "radial_stages %d outside 2..8", radial_stages);
+  ctx->groups[group].mixed.i8.tune_bn = radial_bn;
+  ctx->groups[group].mixed.i8.tune_stages = radial_stages;
+  return GGB_OK;
+}
+
 int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream) {
   if (!ctx) return GGB_ERR_ARG;
   if (phase < 0 || phase > 3) return fail(ctx, GGB_ERR_ARG, "phase %d outside 0..3", phase);

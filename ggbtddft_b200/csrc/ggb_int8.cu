@@ -940,9 +940,10 @@ static size_t a8_smem(int k_atoms, int stages) {
 int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats, std::string& err) {
   const int n_r = a.n_r, n_l = a.n_l;
   I8Group& q = mg.i8;
-  q.bn = r8_bn(a.n_cols);
+  q.bn = q.tune_bn > 0 ? q.tune_bn : r8_bn(a.n_cols);
   q.cols_pad = ((a.n_cols + q.bn - 1) / q.bn) * q.bn;
   q.stages = r8_stages(q.bn);
+  if (q.tune_stages > 0) q.stages = std::min(q.tune_stages, q.stages);
   // W planes and row exponents
   const size_t nw = (size_t)n_l * R8_W_PLANES * mg.rows_pad * mg.k_pad;    // one variant
   I8_CK(cudaMalloc(&q.W, nw * I8_W_VARIANTS));

@@ -29,6 +29,7 @@ struct I8Group {
   int* sexp = nullptr;       // [mat][m][rows]
   CUtensorMap tmW, tmX, tmS;
   int bn = 16, cols_pad = 0, stages = 2, ctas = 0;
+  int tune_bn = 0, tune_stages = 0;   // ggb_set_tuning (0: built-in choice)
   size_t smem = 0;
   int np = 32, a_k_atoms = 0, a_m_tiles = 0, a_stages = 0, a_rows = 0, a_ld = 0;
   size_t a_smem = 0;

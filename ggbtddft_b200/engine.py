@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Dict, List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -52,7 +52,7 @@ _lib = None
 EXPORTS = ("ggb_create", "ggb_set_grid", "ggb_set_radial_propagators", "ggb_set_angular", "ggb_set_orbitals",
            "ggb_set_field", "ggb_step", "ggb_get_step", "ggb_get_observables", "ggb_get_orbitals",
            "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase",
-           "ggb_observables_noalloc")
+           "ggb_set_tuning", "ggb_observables_noalloc")
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -76,6 +76,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_step": ([P, I_, P], I_),
         "ggb_get_step": ([P, ctypes.POINTER(ctypes.c_int)], I_),
         "ggb_launch_phase": ([P, I_, P], I_),
+        "ggb_set_tuning": ([P, I_, I_, I_], I_),
         "ggb_get_observables": ([P, I_, P, P, P, I_, I_], I_),
         "ggb_get_orbitals": ([P, I_, P], I_),
         "ggb_get_potentials": ([P, I_, P, P, P, P], I_),
@@ -117,13 +118,23 @@ class TimePropagation:
     """All runs of an ensemble on one GPU; FP64 parity form or a split-precision form."""
 
     def __init__(self, runs: Sequence[RunInputs], precision: str = "fp64", per_l: bool = True,
-                 n_t: Optional[int] = None, groups: Optional[List[List[int]]] = None, W_device=None):
+                 n_t: Optional[int] = None, groups: Optional[List[List[int]]] = None, W_device=None,
+                 tuning: Optional[Dict[int, Tuple[int, int]]] = None, autotune: bool = False):
+        """``tuning`` = {group: (radial_bn, radial_stages)} (ggb_set_tuning); ``autotune`` = True
+        takes each group's tiles from the autotuner's cache, timing the candidates on a miss
+        (split_int8 form only)."""
         self.lib = load_library()
         self.runs = list(runs)
         self.precision = precision
         self.per_l = per_l
         self.groups = groups if groups is not None else group_runs(self.runs)
         self.n_t = int(n_t if n_t is not None else max(r.n_t for r in self.runs))
+        if autotune and precision == "split_int8" and tuning is None:
+            # before this context allocates anything: the tuner times its candidates in contexts
+            # of its own, one grid group at a time
+            from . import autotune as AT
+            tuning = AT.tuning_for(self.runs, self.groups)
+        self.tuning = tuning
         run_group = {}
         for gi, members in enumerate(self.groups):
             for ri in members:
@@ -152,6 +163,8 @@ class TimePropagation:
                 for m in range(n_m):
                     self._call("ggb_set_angular", gi, cid, m, _ptr(_c(r0.V[c][m], np.float64)),
                                _ptr(_c(r0.D[c][m], np.float64)))
+        for gi, (bn, stages) in (tuning or {}).items():
+            self._call("ggb_set_tuning", int(gi), int(bn), int(stages))
         for i in range(len(self.runs)):
             self.set_orbitals(i, self.runs[i].x0)
             self.set_field(i, self.runs[i].E)

@@ -122,6 +122,14 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream);
    No counterpart in the reference. */
 int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream);
 
+/* Tiles of the int8 radial product of one grid group (split_int8 form; ignored by the others):
+   radial_bn = orbital columns per tile (16, 32 or 64; 0 = the built-in choice from the group's
+   column count), radial_stages = TMA pipeline stages (2..8, capped at what fits in shared memory;
+   0 = the most that fit).  Call before the first ggb_step.  The project's autotuner
+   (ggbtddft_b200/autotune.py) times the candidates for a group's (N_r, l_max, columns) and caches
+   the fastest.  No counterpart in the reference (its radial product is a cuBLAS call). */
+int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages);
+
 /* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */
 int ggb_get_step(ggb_ctx* ctx, int* step);
 
