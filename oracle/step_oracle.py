@@ -189,6 +189,68 @@ class OracleState:
 
     # ----- potentials -----
     def density_multipoles(self, x):
+        """d_getHartreePotentialDensity (hartreePotentialDensity.cuh:1-181): the l ranges and
+        coefficients of density_multipoles_literal, each range summed as one array expression."""
+        p = self.p
+        n_l = p.n_l
+        out = np.zeros((max(p.n_har, 1), p.n_r))
+
+        def xx(a, b, k):
+            """x_a . x_b (real part of conj(x_b) x_a) for index arrays a, b; 0 where out of range."""
+            a, b = np.atleast_1d(a), np.atleast_1d(b)
+            ok = (a >= 0) & (a < n_l) & (b >= 0) & (b < n_l)
+            ac, bc = np.where(ok, a, 0), np.where(ok, b, 0)
+            v = x[ac, k].real * x[bc, k].real + x[ac, k].imag * x[bc, k].imag
+            return np.where(ok[:, None], v, 0.0)
+
+        def rng(lo, hi):
+            return np.arange(lo, hi) if hi > lo else np.zeros(0, dtype=int)
+
+        def term(c, a, b, k):
+            """sum over the range of c[:, None] * xx(a, b)"""
+            if np.size(a) == 0:
+                return 0.0
+            return (np.asarray(c, dtype=np.float64)[:, None] * xx(a, b, k)).sum(axis=0)
+
+        for L in range(p.n_har):
+            tot = np.zeros(p.n_r)
+            for k in range(p.n_kso):
+                m = int(p.m[k])
+                d = np.zeros(p.n_r)
+                if L == 0:
+                    d += (x[m:, k].real ** 2 + x[m:, k].imag ** 2).sum(axis=0)
+                elif L == 1:
+                    lp = rng(m + 1, n_l - 1)
+                    d += term(c_u(np.array([m]), m), [m + 1], [m], k)
+                    d += term(c_u(lp, m), lp + 1, lp, k) + term(c_d(lp, m), lp - 1, lp, k)
+                    d += term(c_d(np.array([n_l - 1]), m), [n_l - 2], [n_l - 1], k)
+                elif L == 2:
+                    lp = rng(m, m + 2)
+                    d += term(q_u(lp, m), lp + 2, lp, k) + term(p_lm(lp, m), lp, lp, k)
+                    lp = rng(m + 2, n_l - 2)
+                    d += (term(q_u(lp, m), lp + 2, lp, k) + term(q_d(lp, m), lp - 2, lp, k)
+                          + term(p_lm(lp, m), lp, lp, k))
+                    lp = rng(n_l - 2, n_l)
+                    d += term(q_d(lp, m), lp - 2, lp, k) + term(p_lm(lp, m), lp, lp, k)
+                elif L == 3:
+                    d += term(p3lm(np.array([m]), m), [m + 1], [m], k) + term(f3lm(np.array([m]), m), [m + 3], [m], k)
+                    lp = rng(m + 1, m + 3)
+                    d += (term(p3lm(lp - 1, m), lp - 1, lp, k) + term(p3lm(lp, m), lp + 1, lp, k)
+                          + term(f3lm(lp, m), lp + 3, lp, k))
+                    lp = rng(m + 3, n_l - 3)
+                    d += (term(f3lm(lp - 3, m), lp - 3, lp, k) + term(p3lm(lp - 1, m), lp - 1, lp, k)
+                          + term(p3lm(lp, m), lp + 1, lp, k) + term(f3lm(lp, m), lp + 3, lp, k))
+                    # the reference's tail loop starts at N_l-4 again (hartreePotentialDensity.cuh:150)
+                    lp = rng(n_l - 4, n_l - 1)
+                    d += (term(f3lm(lp - 3, m), lp - 3, lp, k) + term(p3lm(lp - 1, m), lp - 1, lp, k)
+                          + term(p3lm(lp, m), lp + 1, lp, k))
+                    lp = np.array([n_l - 1])
+                    d += term(f3lm(lp - 3, m), lp - 3, lp, k) + term(p3lm(lp - 1, m), lp - 1, lp, k)
+                tot += float(p.occ[k]) * d
+            out[L] = tot
+        return out
+
+    def density_multipoles_literal(self, x):
         """d_getHartreePotentialDensity (hartreePotentialDensity.cuh:1-181), literal l ranges."""
         p = self.p
         n_l = p.n_l

@@ -75,3 +75,23 @@ def test_oracle_quirk_tail_loop_of_octupole_density():
     # f3lm(3) x3.x6 is counted by the l=3 up-term, the middle loop's l=6 down-term and the tail's
     expect = float(run.occ[0]) * 3 * f3lm(3, 0)
     assert np.allclose(d, expect)
+
+
+@pytest.mark.parametrize("n_l,ms", [(32, [0, 1, 0]), (8, [0, 1, 2]), (5, [0, 1]), (12, [0, 3, 1])])
+def test_density_multipoles_equal_the_literal_loops(n_l, ms):
+    """The array form of the density multipoles sums the same l ranges and coefficients as the
+    literal loops of hartreePotentialDensity.cuh (including the L = 3 tail restart)."""
+    from oracle.step_oracle import OracleState
+
+    class _P:
+        pass
+
+    p = _P()
+    p.n_l, p.n_r, p.n_kso, p.m, p.occ, p.n_har = n_l, 9, len(ms), np.array(ms), np.arange(1, len(ms) + 1), 4
+    st = OracleState.__new__(OracleState)
+    st.p = p
+    rng = np.random.default_rng(n_l)
+    x = rng.standard_normal((n_l, len(ms), 9)) + 1j * rng.standard_normal((n_l, len(ms), 9))
+    a = st.density_multipoles_literal(x)
+    b = st.density_multipoles(x)
+    assert np.abs(a - b).max() <= 1e-14 * np.abs(a).max()
