@@ -114,12 +114,16 @@ def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_int8", n_
     )
 
 
-def compare_ensemble(n_steps: int, precision: str = "split_int8", n_runs: int = 64, seed: int = 0) -> dict:
+def compare_ensemble(n_steps: int, precision: str = "split_int8", n_runs: int = 64, seed: int = 0,
+                     sensitivity: float = 0.0) -> dict:
     """Every instance of the argon focal-scan ensemble: the batched `precision` form (all runs in one
     context, grid groups on concurrent streams) against each run stepped alone in the FP64 form, over
     the first `n_steps` steps of its pulse.  Reports, per instance, the relative L2 difference of the
     total dipole and the largest orbital-norm difference (a window this short has no harmonic
-    spectrum; the full pulses would take hours in the per-instance FP64 form)."""
+    spectrum; the full pulses would take hours in the per-instance FP64 form).  With ``sensitivity``
+    > 0 each run is also stepped in FP64 from orbitals perturbed by that relative amount, and the
+    same two numbers are reported for that pair: the FP64 self-sensitivity of each instance over the
+    same window."""
     runs = P.argon_ensemble(n_runs, seed=seed, n_steps=n_steps, device="cuda")
     tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_steps)
     done = 0
@@ -134,16 +138,25 @@ def compare_ensemble(n_steps: int, precision: str = "split_int8", n_runs: int = 
         ref = _run(r, "fp64", n_steps)
         d_ref = S.total_dipole(ref["dipole"], r.l_active, r.m_active, r.occ)
         d_tst = S.total_dipole(tst["dipole"], r.l_active, r.m_active, r.occ)
-        per.append(dict(run=i, n_r=r.n_r, l_max=r.n_l - 1,
-                        dipole_rel_l2=float(np.linalg.norm(d_tst - d_ref) / np.linalg.norm(d_ref)),
-                        norm_drift_max=float(np.abs(tst["norm"] - ref["norm"]).max()),
-                        fp64_status=ref["status"][0]))
+        row = dict(run=i, n_r=r.n_r, l_max=r.n_l - 1,
+                   dipole_rel_l2=float(np.linalg.norm(d_tst - d_ref) / np.linalg.norm(d_ref)),
+                   norm_drift_max=float(np.abs(tst["norm"] - ref["norm"]).max()),
+                   fp64_status=ref["status"][0])
+        if sensitivity > 0:
+            pert = _run(perturb_orbitals(r, sensitivity), "fp64", n_steps)
+            d_p = S.total_dipole(pert["dipole"], r.l_active, r.m_active, r.occ)
+            row["fp64_self_dipole_rel_l2"] = float(np.linalg.norm(d_p - d_ref) / np.linalg.norm(d_ref))
+            row["fp64_self_norm_drift_max"] = float(np.abs(pert["norm"] - ref["norm"]).max())
+        per.append(row)
     tp.close()
     return dict(config=f"argon ensemble, {n_runs} runs (seed {seed})", precision=precision, steps=n_steps,
                 batched_status=batched_status, per_instance=per,
                 dipole_rel_l2_max=max(q["dipole_rel_l2"] for q in per),
                 dipole_rel_l2_median=float(np.median([q["dipole_rel_l2"] for q in per])),
-                norm_drift_max=max(q["norm_drift_max"] for q in per))
+                norm_drift_max=max(q["norm_drift_max"] for q in per),
+                fp64_self_sensitivity=None if sensitivity <= 0 else dict(
+                    eps=sensitivity, dipole_rel_l2_max=max(q["fp64_self_dipole_rel_l2"] for q in per),
+                    dipole_rel_l2_median=float(np.median([q["fp64_self_dipole_rel_l2"] for q in per]))))
 
 
 CONFIGS = {
@@ -167,7 +180,7 @@ def main(argv=None):
                          "FP64, over this many steps")
     args = ap.parse_args(argv)
     if args.ensemble_steps > 0:
-        rep = compare_ensemble(args.ensemble_steps, args.precision)
+        rep = compare_ensemble(args.ensemble_steps, args.precision, sensitivity=args.sensitivity)
         if args.out:
             with open(args.out, "w") as f:
                 f.write(json.dumps(rep) + "\n")
