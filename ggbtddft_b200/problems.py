@@ -268,7 +268,7 @@ def quiver_radius(laser: LaserSpec) -> float:
 
 
 def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = None, device=None,
-                   ladder: Sequence[GridRung] = ARGON_LADDER) -> List[RunInputs]:
+                   ladder: Sequence[GridRung] = ARGON_LADDER, only=None) -> List[RunInputs]:
     """Argon LDA in-situ focal scan: I ~ U[0.8, 2]e14 W/cm^2, lambda ~ U[800, 1300] nm, 10-cycle sin^2,
     dt = 0.02, 9 orbitals; each run goes on the ladder rung indexed by its wavelength
     (longer wavelength -> larger excursion and higher cutoff -> larger grid and l_max)."""
@@ -276,11 +276,11 @@ def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = Non
     I0 = rng.uniform(0.8e14, 2.0e14, n_runs)
     lam = rng.uniform(800.0, 1300.0, n_runs)
     return _ensemble("Ar", I0, lam, np.zeros(n_runs), 10.0, 0.02, n_steps, device, ladder,
-                     lambda l: min(len(ladder) - 1, int((l - 800.0) / 100.0)))
+                     lambda l: min(len(ladder) - 1, int((l - 800.0) / 100.0)), only=only)
 
 
 def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None, device=None,
-                 ladder: Sequence[GridRung] = HHE_LADDER) -> List[RunInputs]:
+                 ladder: Sequence[GridRung] = HHE_LADDER, only=None) -> List[RunInputs]:
     """H/He-like scan: I log-uniform in [0.5, 3]e14, CEP ~ U[0, 2 pi), lambda ~ U[800, 1800] nm,
     6-cycle sin^2, dt = 0.03; atoms alternate H / He; the rung is the smallest whose r_max covers
     3 quiver radii plus the absorber."""
@@ -296,15 +296,19 @@ def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None
                 return k
         return len(ladder) - 1
     atoms = ["H" if i % 2 == 0 else "He" for i in range(n_runs)]
-    return _ensemble(atoms, I0, lam, cep, 6.0, 0.03, n_steps, device, ladder, None, rung_of_run=rung)
+    return _ensemble(atoms, I0, lam, cep, 6.0, 0.03, n_steps, device, ladder, None, rung_of_run=rung, only=only)
 
 
-def _ensemble(atom, I0, lam, cep, cycles, dt, n_steps, device, ladder, rung_of_lambda, rung_of_run=None):
+def _ensemble(atom, I0, lam, cep, cycles, dt, n_steps, device, ladder, rung_of_lambda, rung_of_run=None,
+              only=None):
+    """The runs of an ensemble from its drawn parameters; ``only`` = indices of the runs to build
+    (the draws are made for the whole ensemble first, so a selected run equals its twin in the full
+    ensemble)."""
     n_runs = len(I0)
     runs: List[RunInputs] = []
     gs_cache: dict = {}
     w_cache: dict = {}
-    for i in range(n_runs):
+    for i in (range(n_runs) if only is None else only):
         a = atom[i] if isinstance(atom, list) else atom
         k = rung_of_run(i) if rung_of_run is not None else rung_of_lambda(lam[i])
         g = ladder[k]
