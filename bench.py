@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -124,10 +125,10 @@ def read_peaks():
 class ClockSampler:
     """nvidia-smi clocks/throttle sampling during the timed region."""
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, path: str = None):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+        self.path = path or os.path.join(tempfile.mkdtemp(prefix="ggb_clocks_"), f"clocks_gpu{index}.csv")
 
     def __enter__(self):
         try:
@@ -268,7 +269,7 @@ def run_ours(args, rank, world, dist):
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
+    with ClockSampler(dev, args.clocks_csv) as clk:
         e0.record(stream)
         tp.step(args.steps, h)
         e1.record(stream)
@@ -430,6 +431,8 @@ def main():
     ap.add_argument("--precision", default="split_int8", choices=["split_int8", "split_bf16"],
                     help="form of the split-precision workloads (FP64 workloads end in -fp64)")
     ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--clocks-csv", default=None,
+                    help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")
     ap.add_argument("--compare-fp64", type=int, default=1,
                     help="also time the runs one at a time in the FP64 form (per-instance baseline)")

@@ -159,6 +159,67 @@ def compare_ensemble(n_steps: int, precision: str = "split_int8", n_runs: int = 
                     dipole_rel_l2_median=float(np.median([q["fp64_self_dipole_rel_l2"] for q in per]))))
 
 
+def _run_totals(run: P.RunInputs, n_steps: int, chunk: int = 8192):
+    """FP64 form, one run, totals over l only (per-l series of long fine-step runs would take GBs)."""
+    tp = TimePropagation([run], precision="fp64", per_l=False, n_t=n_steps)
+    t0 = time.perf_counter()
+    done = 0
+    while done < n_steps:
+        k = min(chunk, n_steps - done)
+        tp.step(k)
+        done += k
+    obs = tp.observables(0, per_l=False, n_steps=n_steps)
+    st, msg = tp.status()
+    tp.close()
+    d = (run.occ[:, None] * obs["dipole"].real).sum(axis=0)
+    return dict(dipole=d, norm=obs["norm"], seconds=time.perf_counter() - t0, status=(st, msg))
+
+
+def sensitivity_sweep(variants=((0.02, 4), (0.01, 4), (0.005, 4), (0.02, 3), (0.02, 2)), eps: float = 1e-10,
+                      windows: int = 10) -> dict:
+    """Where the argon LDA self-sensitivity comes from: for each (dt, N_har) the FP64 form is run twice
+    over the whole pulse (same physical time), from the ground state and from it perturbed by ``eps``,
+    and the growth of the difference is recorded per tenth of the pulse.  A growth rate that falls
+    with dt is a property of the time stepping (potentials lagging one step behind the orbitals);
+    one that does not is a property of the equations.  N_har = 2 keeps only the dipole Hartree term
+    (the S phase, which carries the monopole Hartree and exchange changes, runs only for N_har >= 3;
+    couplingS.cuh:49), N_har = 3 adds S and the quadrupole, N_har = 4 the octupole.
+    Also reported: the dipole of each finer step against the dt = 0.02 run at the common times
+    (time-step convergence of the trajectory itself)."""
+    laser = P.LaserSpec(1.4e14, 800.0, 10.0, 0.0)
+    gs_cache: dict = {}
+    rows, by_dt = [], {}
+    for dt, n_har in variants:
+        run = P.baseline_run("Ar", 600, 300.0, 96, dt, laser, 60.0, device="cuda", gs_cache=gs_cache)
+        run = dataclasses.replace(run, n_har=n_har, name=f"{run.name}-dt{dt}-nhar{n_har}")
+        n = run.n_t
+        ref = _run_totals(run, n)
+        pert = _run_totals(perturb_orbitals(run, eps), n)
+        d_r, d_p = ref["dipole"], pert["dipole"]
+        scale = float(np.abs(d_r).max())
+        edges = np.linspace(0, n, windows + 1).astype(int)
+        growth = [float(np.abs(d_p[a:b] - d_r[a:b]).max() / scale) for a, b in zip(edges[:-1], edges[1:])]
+        rows.append(dict(dt=dt, n_har=n_har, steps=n, seconds=ref["seconds"] + pert["seconds"],
+                         status=[ref["status"][0], pert["status"][0]], eps=eps,
+                         diff_per_tenth_of_pulse=growth,
+                         dipole_rel_l2=float(np.linalg.norm(d_p - d_r) / np.linalg.norm(d_r)),
+                         norm_diff_max=float(np.abs(pert["norm"] - ref["norm"]).max())))
+        if n_har == 4:
+            by_dt[dt] = d_r
+    conv = {}
+    if 0.02 in by_dt:
+        base = by_dt[0.02]
+        for dt, d in by_dt.items():
+            if dt == 0.02:
+                continue
+            k = int(round(0.02 / dt))
+            sub = d[k - 1::k][:base.size]
+            m = min(sub.size, base.size)
+            conv[str(dt)] = float(np.linalg.norm(sub[:m] - base[:m]) / np.linalg.norm(base[:m]))
+    return dict(config="Ar LDA, N_r 600, r_max 300, l_max 96, 800 nm 1.4e14 10-cycle sin^2", variants=rows,
+                dipole_vs_dt002_rel_l2=conv)
+
+
 CONFIGS = {
     "hydrogen": ("H", P.config_hydrogen),
     "helium": ("He", P.config_helium),
@@ -178,7 +239,17 @@ def main(argv=None):
     ap.add_argument("--ensemble-steps", type=int, default=0,
                     help="instead: every run of the 64-run argon ensemble, batched, against each run alone in "
                          "FP64, over this many steps")
+    ap.add_argument("--sweep", action="store_true",
+                    help="instead: FP64 self-sensitivity of argon LDA for dt in {0.02, 0.01, 0.005} and N_har "
+                         "in {2, 3, 4} over the whole pulse")
     args = ap.parse_args(argv)
+    if args.sweep:
+        rep = sensitivity_sweep(eps=args.sensitivity or 1e-10)
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(rep) + "\n")
+        print(json.dumps(rep))
+        return
     if args.ensemble_steps > 0:
         rep = compare_ensemble(args.ensemble_steps, args.precision, sensitivity=args.sensitivity)
         if args.out:

@@ -5,8 +5,9 @@ bn (orbital columns per tile: 16, 32 or 64) and the number of TMA pipeline stage
 in shared memory).  The library's built-in choice takes bn from the group's column count and the
 most stages that fit.  The tuner times every candidate on the group's own runs (the radial phase
 launched alone, CUDA events, after warm-up) and keeps the fastest.  Results are cached in a JSON
-file keyed on the GPU's name and the group's (N_r, l_max, orbital columns), so a grid shape is timed
-once per GPU model; the cache is $GGB_AUTOTUNE_CACHE, else ~/.cache/ggbtddft_b200/autotune.json.
+file keyed on the GPU's name, the library version and the group's (N_r, l_max, orbital columns), so
+a grid shape is timed once per GPU model and kernel version; the cache is $GGB_AUTOTUNE_CACHE, else
+~/.cache/ggbtddft_b200/autotune.json.
 
     TimePropagation(runs, precision="split_int8", autotune=True)   # cached or tuned tiles
     tuning_for(runs, groups)                                         # {group: (bn, stages)}
@@ -32,12 +33,31 @@ def max_stages(bn: int) -> int:
     return max(2, min(8, SMEM_BUDGET // stage))
 
 
+# Every k_radial_i8 CTA allocates 512 tensor-memory columns (all of an SM's).  A CTA whose shared
+# memory leaves room for a second one on its SM (<= 113 KB of the SM's 228 KB, with the 1 KB the
+# runtime reserves per CTA) can be placed beside another radial CTA -- of its own grid or of another
+# grid group's concurrent launch -- which then waits in tcgen05.alloc until the first one exits.
+# Timed alone such a tile looks fine and is slower in the real step, so it is not a candidate.
+SM_SMEM = 228 * 1024
+CTA_RESERVED = 1024
+
+
+def smem_bytes(bn: int, stages: int) -> int:
+    """Dynamic shared memory of one k_radial_i8 CTA (the library's r8_smem)."""
+    return stages * (R8_W_PLANES * R8_BM * R8_BK + R8_X_PLANES * bn * R8_BK) + 1024
+
+
+def one_cta_per_sm(bn: int, stages: int) -> bool:
+    return 2 * (smem_bytes(bn, stages) + CTA_RESERVED) > SM_SMEM
+
+
 def candidates(n_cols: int) -> List[Tuple[int, int]]:
     """(bn, stages) pairs worth timing: tile widths up to the first one that covers all columns
-    (a wider tile only adds padding), each with 2 .. max_stages(bn) stages."""
+    (a wider tile only adds padding), each with the stage counts from 2 to max_stages(bn) whose
+    shared memory keeps one CTA per SM."""
     out = []
     for bn in BN_CHOICES:
-        out.extend((bn, st) for st in range(2, max_stages(bn) + 1))
+        out.extend((bn, st) for st in range(2, max_stages(bn) + 1) if one_cta_per_sm(bn, st))
         if bn >= n_cols:
             break
     return out
@@ -48,8 +68,18 @@ def cache_path() -> str:
         os.path.expanduser("~"), ".cache", "ggbtddft_b200", "autotune.json")
 
 
-def cache_key(n_r: int, l_max: int, n_cols: int, device_name: str) -> str:
-    return f"{device_name}|N_r={n_r}|l_max={l_max}|cols={n_cols}"
+def library_version() -> str:
+    """ggb_version() of the loaded library, so that tunings of older kernels are not reused."""
+    try:
+        from .engine import load_library
+        return load_library().ggb_version().decode()
+    except Exception:
+        return "unknown"
+
+
+def cache_key(n_r: int, l_max: int, n_cols: int, device_name: str, version: Optional[str] = None) -> str:
+    v = library_version() if version is None else version
+    return f"{device_name}|{v}|N_r={n_r}|l_max={l_max}|cols={n_cols}"
 
 
 def load_cache(path: str) -> Dict[str, dict]:

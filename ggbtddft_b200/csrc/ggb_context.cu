@@ -602,6 +602,8 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream) {
 int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages) {
   if (!ctx) return GGB_ERR_ARG;
   if (group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, GGB_ERR_ARG, "group %d out of range", group);
+  if (ctx->dims.precision != GGB_SPLIT_INT8)
+    return fail(ctx, GGB_ERR_STATE, "ggb_set_tuning applies to the split_int8 form only");
   if (ctx->prepared) return fail(ctx, GGB_ERR_STATE, "ggb_set_tuning after the first ggb_step");
   if (radial_bn != 0 && radial_bn != 16 && radial_bn != 32 && radial_bn != 64)
     return fail(ctx, GGB_ERR_ARG, "radial_bn %d is not 0, 16, 32 or 64", radial_bn);

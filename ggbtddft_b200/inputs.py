@@ -145,7 +145,7 @@ def cap_manolopoulos(r: np.ndarray, r_mask: float, r_max: float) -> np.ndarray:
 def mask_cos8(r: np.ndarray, r_max: float, width: float) -> np.ndarray:
     """Multiplicative absorbing mask cos^(1/8)(pi/2 (r - r0)/width) over the last ``width`` a.u.
 
-    Not in the reference (which folds a CAP into W); the BASELINE configurations ask for it.
+    Not in the reference (which folds a CAP into W); the benchmark configurations use it.
     Applied once per radial step, folded into the radial propagator rows: W' = diag(mask) W.
     """
     r0 = r_max - width
@@ -400,7 +400,7 @@ def field_sin2(n_t: int, dt: float, e0: float, omega0: float, n_cycles: float, c
     """sin^2-envelope pulse of n_cycles optical cycles sampled at t_k = k dt, k = 0..n_t-1.
 
     E(t) = E0 sin^2(pi t / T) cos(w0 (t - T/2) + CEP) for 0 <= t <= T = n_cycles 2 pi / w0, 0 after.
-    Not in the reference (which uses a super-Gaussian); the BASELINE configurations ask for it.
+    Not in the reference (which uses a super-Gaussian); the benchmark configurations use it.
     """
     t = np.arange(n_t) * dt
     T = n_cycles * 2.0 * np.pi / omega0

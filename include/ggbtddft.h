@@ -34,8 +34,8 @@ enum {
   GGB_FP64 = 0,        /* complex128 orbitals, FP64 arithmetic: parity form                         */
   GGB_SPLIT_BF16 = 1,  /* complex64 orbitals, 3xBF16 split products on tcgen05, FP32 accumulation    */
   GGB_SPLIT_TF32 = 2,  /* reserved: 3xTF32 split products (not built; ggb_create returns GGB_ERR_ARG) */
-  GGB_SPLIT_INT8 = 3   /* complex64 orbitals, four int8 slices per operand on tcgen05 (kind::i8),
-                          exact int32 accumulation: the form that holds the long-pulse error bound   */
+  GGB_SPLIT_INT8 = 3   /* complex128 orbitals; the products' operands are cut into four int8 slices
+                          on tcgen05 (kind::i8) with exact int32 accumulation: the fast form         */
 };
 
 /* angular couplings (workingData/hamiltonian/propagatorsL/<dir>):  P 001/001, FP 001/003,
@@ -60,7 +60,8 @@ enum {
 /* A grid group: runs that share the radial grid, N_l and the radial propagators W_l. */
 typedef struct ggb_group_desc {
   int n_r;      /* radial points N_r (any value >= 2; no multiple-of-32 restriction)       */
-  int n_l;      /* angular momenta N_l = l_max + 1 (<= 220)                                 */
+  int n_l;      /* angular momenta N_l = l_max + 1 (2 .. 220 in every form: two [N_l][32]
+                   complex128 tiles of the FP64 angular kernel fit in shared memory)           */
   int n_m;      /* number of azimuthal blocks N_m (m = 0 .. n_m-1)                          */
 } ggb_group_desc;
 
@@ -122,12 +123,13 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream);
    No counterpart in the reference. */
 int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream);
 
-/* Tiles of the int8 radial product of one grid group (split_int8 form; ignored by the others):
+/* Tiles of the int8 radial product of one grid group (split_int8 form only):
    radial_bn = orbital columns per tile (16, 32 or 64; 0 = the built-in choice from the group's
    column count), radial_stages = TMA pipeline stages (2..8, capped at what fits in shared memory;
    0 = the most that fit).  Call before the first ggb_step.  The project's autotuner
    (ggbtddft_b200/autotune.py) times the candidates for a group's (N_r, l_max, columns) and caches
-   the fastest.  No counterpart in the reference (its radial product is a cuBLAS call). */
+   the fastest.  Returns GGB_ERR_STATE for a context of another form.  No counterpart in the
+   reference (its radial product is a cuBLAS call). */
 int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages);
 
 /* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */

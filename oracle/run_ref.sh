@@ -3,7 +3,8 @@
 # Test infrastructure only.  Usage (on a GPU machine, from the repository root):
 #   bash oracle/run_ref.sh <dest>      # copies <case>/output and the console log to <dest>/<case>/
 set -euo pipefail
-dest=${1:-gpurun_out/ref}
+if [ $# -ne 1 ]; then echo "usage: bash oracle/run_ref.sh <dest>" >&2; exit 2; fi
+dest=$1
 root=$(cd "$(dirname "$0")" && pwd)/_ref
 for d in "$root"/*/; do
   [ -x "$d/ggb_ref" ] || continue

@@ -37,4 +37,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/ref")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_ref_fixtures.py <dir written by oracle/run_ref.sh>")
+    main(sys.argv[1])
