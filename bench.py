@@ -96,13 +96,25 @@ def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8", o
     raise SystemExit(f"unknown workload {name}")
 
 
+def workload_groups(name: str):
+    """[(representative run index, runs in the group, label)] for the grid groups of a workload, without
+    building its runs: the CPU legs time one run per group and weight it by the group's size."""
+    from ggbtddft_b200 import problems as P
+    if name.startswith("ar-ens64") or name.startswith("hhe-ens256"):
+        dr = P.argon_draws(64, seed=0) if name.startswith("ar-ens64") else P.hhe_draws(256, seed=0)
+        out = []
+        for (k, atom), members in dr.grid_groups().items():
+            g = dr.ladder[k]
+            out.append((members[0], len(members), f"{atom} N_r {g.n_r} l_max {g.l_max}"))
+        return out
+    runs = {"ar16-n600": 16, "ar16-n400-l160": 16}.get(name, 1)
+    return [(0, runs, name)]
+
+
 DEFAULT_WORKLOAD = "ar-ens64"
 # tensor-core products executed per algorithmic real product, and the peak they run against
 SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (BF16)
                   "split_int8": 10}   # int8 slice pairs (j, m), 0-based, with j + m <= 3
-# dense int8 tensor throughput is twice the bf16 throughput on B200 (4.5 vs 2.25 POPS nominal); the
-# int8 roofline takes twice the measured bf16 figure
-TENSOR_PEAK_FACTOR = {"split_bf16": 1.0, "split_int8": 2.0}
 W_BYTES = {"fp64": 16, "split_bf16": 12, "split_int8": 8}   # per complex element of W as streamed
 # kernels launched per grid group and step: fp64 angular, radial, angular (+ partials), finalize;
 # split_bf16 angular, radial, angular, partials, finalize; split_int8 angular, operand slicing,
@@ -120,6 +132,13 @@ def read_peaks():
         d = json.load(open(p))
         return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
     return 6650.0, 1590.0, "fallback"
+
+
+def compute_peaks(stream_handle):
+    """FP64 FMA and tcgen05 int8 peaks of this GPU from the library's own microbenchmarks
+    (ggb_measure_peaks), taken once before the timed region."""
+    from ggbtddft_b200.engine import measure_peaks
+    return measure_peaks(stream_handle)
 
 
 class ClockSampler:
@@ -261,6 +280,7 @@ def run_ours(args, rank, world, dist):
     stream = torch.cuda.Stream()
     h = stream.cuda_stream
     hbm_peak, _, peak_kind = read_peaks()
+    peaks = compute_peaks(h)
 
     # warm-up (also captures the step graph)
     tp.step(args.warmup, h)
@@ -319,21 +339,28 @@ def run_ours(args, rank, world, dist):
         tp2.close()
         e2e_value = world * units_per_step * args.steps / e2e_s
 
-    # roofline of the dominant kernel (the phase with the longest device time per step): the HBM
-    # bound (algorithmic bytes) and, for the split forms, the tensor bound (executed split products)
-    # are both evaluated and the larger fraction is reported; every phase's figures stay in `kernels`
+    # roofline of the dominant kernel (the phase with the longest device time per step), by the
+    # algorithmic bytes and flops of each phase: frac = max(bytes / t / HBM peak, flops / t / the
+    # precision's peak).  The peaks of the arithmetic are this GPU's, measured by the library's own
+    # microbenchmarks before the timed region; the HBM peak is the measured copy bandwidth.  The int8
+    # form's executed slice products (10 per algorithmic real product) are a secondary figure.
     tf = phase_traffic(runs, tp.groups, precision)
     dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
-    tensor_peak = read_peaks()[1] * TENSOR_PEAK_FACTOR[precision] if precision != "fp64" else None
+    arith_peak = {"fp64": peaks["fp64_tflops"], "split_int8": peaks["int8_tops"],
+                  "split_bf16": read_peaks()[1]}[precision]
+    arith_unit = {"fp64": "TFLOP/s (FP64 FMA)", "split_int8": "TOP/s (tcgen05 kind::i8)",
+                  "split_bf16": "TFLOP/s (bf16, cuBLAS-measured)"}[precision]
     sp = SPLIT_PRODUCTS.get(precision, 1)
     kernels = {}
     for k in ("radial", "angular_first", "angular_second"):
         sec = phase_ms[k] / 1e3
         kernels[k] = dict(ms=round(phase_ms[k], 5), algorithmic_bytes=int(tf[k]["bytes"]),
+                          algorithmic_flops=int(tf[k]["flops"]),
                           gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3),
-                          hbm_frac=round(tf[k]["bytes"] / sec / 1e9 / hbm_peak, 4))
-        if tensor_peak:
-            kernels[k]["tensor_frac_executed"] = round(sp * tf[k]["flops"] / sec / 1e12 / tensor_peak, 4)
+                          hbm_frac=round(tf[k]["bytes"] / sec / 1e9 / hbm_peak, 4),
+                          arith_frac=round(tf[k]["flops"] / sec / 1e12 / arith_peak, 4))
+        if precision != "fp64":
+            kernels[k]["tensor_frac_executed"] = round(sp * tf[k]["flops"] / sec / 1e12 / arith_peak, 4)
     kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
     names = {"radial": {"fp64": "k_radial_fp64", "split_bf16": "k_radial_tc_persistent (tcgen05 kind::f16)",
                         "split_int8": "k_radial_i8 (tcgen05 kind::i8, int8 slices, int32 accumulation)"},
@@ -345,18 +372,33 @@ def run_ours(args, rank, world, dist):
     roofline = dict(bound="hbm", kernel=f"{dom} ({kname})", achieved=d["gbs"], peak=hbm_peak, unit="GB/s",
                     frac=d["hbm_frac"], traffic=None if est is None else int(est),
                     traffic_source=None if est is None else TRAFFIC_SOURCE,
-                    peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom, kernels=kernels)
-    if tensor_peak and d["tensor_frac_executed"] > d["hbm_frac"]:
-        pk = f"{peak_kind} bf16_tflops" + (" x2 (int8)" if precision == "split_int8" else "")
-        roofline.update(bound="tensor", achieved=round(sp * d["tflops"], 3), peak=round(tensor_peak, 1),
-                        unit="TFLOP/s (executed split products)" if precision == "split_bf16"
-                        else "TOP/s (executed int8 slice products)",
-                        frac=d["tensor_frac_executed"], peak_kind=pk)
-    # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU
+                    peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom,
+                    peaks_measured=dict(hbm_gbs=hbm_peak, fp64_tflops=round(peaks["fp64_tflops"], 2),
+                                        int8_tops=round(peaks["int8_tops"], 1),
+                                        how="FP64 FMA and tcgen05 kind::i8 microbenchmarks of this library "
+                                            "(ggb_measure_peaks); HBM: copy bandwidth of MEASURED_PEAKS.json"),
+                    kernels=kernels)
+    if d["arith_frac"] > d["hbm_frac"]:
+        roofline.update(bound="tensor" if precision != "fp64" else "fp64", achieved=d["tflops"],
+                        peak=round(arith_peak, 2), unit=arith_unit, frac=d["arith_frac"],
+                        peak_kind="measured (ggb_measure_peaks)")
+    if precision != "fp64":
+        roofline["tensor_frac_executed"] = d["tensor_frac_executed"]
+    # the whole step against its own bound: algorithmic bytes and flops of all phases
+    step_bytes = sum(tf[k]["bytes"] for k in tf)
+    step_flops = sum(tf[k]["flops"] for k in tf)
+    step_s = ms_max / args.steps / 1e3 / world
+    roofline["step"] = dict(ms=round(ms_max / args.steps, 4), algorithmic_bytes=int(step_bytes),
+                            algorithmic_flops=int(step_flops),
+                            bound_ms=round(1e3 * max(step_bytes / (hbm_peak * 1e9), step_flops / (arith_peak * 1e12)), 4),
+                            frac=round(max(step_bytes / (hbm_peak * 1e9), step_flops / (arith_peak * 1e12)) / step_s, 4))
+    # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU,
+    # with that form's own roofline (its step's algorithmic bytes and flops against the HBM and the
+    # measured FP64 peak)
     fp64_inst = None
     if args.compare_fp64 and (len(runs) > 1 or precision != "fp64"):
         from ggbtddft_b200.engine import group_runs
-        total_s, units = 0.0, 0
+        total_s, units, bound_s = 0.0, 0, 0.0
         for members in group_runs(runs):
             one = TimePropagation([runs[members[0]]], precision="fp64", per_l=True, n_t=n_t)
             one.step(args.warmup, h)
@@ -368,12 +410,19 @@ def run_ours(args, rank, world, dist):
             torch.cuda.synchronize()
             per_step = a.elapsed_time(b) / 1e3 / k
             one.close()
+            t1 = phase_traffic([runs[members[0]]], [[0]], "fp64")
+            by = sum(t1[q]["bytes"] for q in t1)
+            fl = sum(t1[q]["flops"] for q in t1)
+            bound_s += len(members) * max(by / (hbm_peak * 1e9), fl / (peaks["fp64_tflops"] * 1e12))
             total_s += per_step * len(members)
             units += sum(runs[i].n_orb for i in members)
         rate = units / total_s
         fp64_inst = dict(value=rate, unit="orbital-steps/s",
                          how="each run of the workload stepped alone in the FP64 form (one time per grid, "
-                             "weighted by the runs on it), same GPU", speedup=round(value / rate, 2))
+                             "weighted by the runs on it), same GPU", speedup=round(value / rate, 2),
+                         roofline_frac=round(bound_s / total_s, 4),
+                         roofline_how="per run-step: max(algorithmic bytes / HBM peak, algorithmic flops / "
+                                      "measured FP64 peak) over the measured time, weighted like the rate")
     return dict(value=value, ms=ms_max, units_per_step=units_per_step, desc=desc, precision=precision,
                 clocks=clk.summary(), roofline=roofline,
                 e2e=None if e2e_value is None else dict(
@@ -384,7 +433,7 @@ def run_ours(args, rank, world, dist):
 
 
 def cpu_port_rate(runs, n_steps: int, warmup: int = 1):
-    """Orbital-steps/s of the CPU oracle on ``n_steps`` steps of the first run."""
+    """Orbital-steps/s and seconds of the CPU oracle on ``n_steps`` steps of the first of ``runs``."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle.step_oracle import OracleProblem, OracleState
     r = runs[0]
@@ -402,21 +451,39 @@ def cpu_port_rate(runs, n_steps: int, warmup: int = 1):
     return r.n_orb * n_steps / dt, dt
 
 
-# the reference arm's bounded sample: at most this many timed steps of the first run (a step of one
-# run is a sample of the workload's step), after at most two warm-up steps
-REF_SAMPLE_STEPS = 40
+def cpu_workload_rate(name: str, n_steps: int, warmup: int):
+    """The CPU oracle on a bounded sample of the workload: one run per grid group, ``n_steps`` timed
+    steps each (after ``warmup``), weighted by the runs in its group.  Returns (orbital-steps/s of the
+    whole workload, seconds timed, estimated CPU seconds of one whole-workload step, sample text, the
+    workload's description)."""
+    units, step_s, timed, parts, desc = 0.0, 0.0, 0.0, [], None
+    for idx, count, label in workload_groups(name):
+        runs, _, desc = workload_runs(name, n_steps + warmup + 8, only=[idx])
+        runs = runs[:1] if idx == 0 else runs
+        rate, sec = cpu_port_rate(runs, n_steps, warmup)
+        per_step = sec / n_steps
+        units += count * runs[0].n_orb
+        step_s += count * per_step
+        timed += sec
+        parts.append(f"{label} (run {idx}, weight {count}): {1e3 * per_step:.0f} ms/step")
+    text = (f"oracle (FP64 NumPy restatement of the reference loop), one run per grid group, {n_steps} steps "
+            f"each after {warmup} warm-up, weighted by the runs per group; " + "; ".join(parts))
+    return units / step_s, timed, step_s, text, desc
+
+
+# the reference arm's bounded sample: at most this many timed steps per grid group, after at most two
+# warm-up steps
+REF_SAMPLE_STEPS = 6
 
 
 def run_reference(args, rank, world):
     """CPU arm: the oracle (FP64 NumPy restatement of the reference loop) on the host cores, on a
-    bounded sample of the workload (the first run; only that run's inputs are built)."""
+    bounded sample of the workload (one run per grid group, weighted by the group's runs)."""
     if rank != 0:
         return None
     n, w = min(args.steps, REF_SAMPLE_STEPS), min(args.warmup, 2)
-    runs, precision, desc = workload_runs(args.workload, n + w + 8, only=[0])
-    rate, dt = cpu_port_rate(runs, n, warmup=w)
-    return dict(value=rate, desc=desc, seconds=dt, steps_timed=n,
-                sample=f"run 0 of the workload, {n} steps after {w} warm-up, {dt:.1f} s")
+    rate, timed, step_s, text, desc = cpu_workload_rate(args.workload, n, w)
+    return dict(value=rate, desc=desc, seconds=timed, step_seconds=step_s, steps_timed=n, sample=text)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -430,7 +497,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split_int8", choices=["split_int8", "split_bf16"],
                     help="form of the split-precision workloads (FP64 workloads end in -fp64)")
-    ap.add_argument("--cpu-sample-steps", type=int, default=20)
+    ap.add_argument("--cpu-sample-steps", type=int, default=4,
+                    help="oracle steps timed per grid group for cpu_baseline (0: skip)")
     ap.add_argument("--clocks-csv", default=None,
                     help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")
@@ -449,7 +517,7 @@ def main():
         res = run_reference(args, rank, world)
         if rank == 0:
             line = dict(metric=metric, value=res["value"], unit="orbital-steps/s", n_gpus=args.gpus,
-                        steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * res["seconds"] / res["steps_timed"],
+                        steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * res["step_seconds"],
                         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
                         data="synthetic (seeded laser parameters; LDA ground state computed at set-up)",
                         config=dict(res["desc"], l2="n/a (CPU)"), impl="reference",
@@ -466,12 +534,8 @@ def main():
     res = run_ours(args, rank, world, dist)
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_steps > 0:
-        n_t = args.cpu_sample_steps + 4
-        runs, _, wdesc = workload_runs(args.workload, n_t, only=[0])
-        rate, dt = cpu_port_rate(runs, args.cpu_sample_steps)
-        cpu = dict(value=rate, unit="orbital-steps/s", cores=cores, kind="port",
-                   sample=f"oracle (FP64 NumPy restatement of the reference loop), run 0 of "
-                          f"{wdesc.get('runs', 1)}, {args.cpu_sample_steps} steps, {dt:.1f} s")
+        rate, timed, _, text, _ = cpu_workload_rate(args.workload, args.cpu_sample_steps, 1)
+        cpu = dict(value=rate, unit="orbital-steps/s", cores=cores, kind="port", sample=f"{text}; {timed:.1f} s timed")
     if rank == 0:
         desc = dict(res["desc"])
         desc["l2"] = "inputs larger than L2 (radial propagators stream from HBM every step)"

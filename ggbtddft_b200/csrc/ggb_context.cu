@@ -45,7 +45,7 @@ struct GroupHost {
   GroupArgs args{};
   MixedGroup mixed;              // split-precision form (ggb_mixed.cu)
   // flags shared by the runs of the group
-  int n_har = 0, use_hartree = 0, target_id = 0;
+  int n_har = 0, use_hartree = 0, target_id = 0, theta = 0;
   double dt = 0.0;
 };
 
@@ -70,9 +70,11 @@ struct ggb_ctx {
   bool prepared = false;
   std::string err;
   int device = 0;
-  // graph of `graph_steps` steps
+  // graphs of `graph_steps` steps and of one step: a call of n steps replays the first n / 32 times
+  // and the second n % 32 times, so every step runs from a graph
   int graph_steps = 32;
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph1_exec = nullptr;
   cudaStream_t cap_stream = nullptr;
   // one stream per grid group (groups share no buffers, so their steps run concurrently), with the
   // events that fork them from and join them to the caller's stream
@@ -188,6 +190,11 @@ struct Act {
 static std::vector<Act> active_couplings(const GroupHost& g) {
   const bool h = g.use_hartree == 1 && g.target_id > 0;
   std::vector<Act> a;
+  if (g.theta) {
+    // the theta form: the P coupling's eigenbasis only, with the whole angular potential in its phase
+    a.push_back({GGB_COUPLING_P, PH_THETA});
+    return a;
+  }
   if (h && g.n_har >= 4) a.push_back({GGB_COUPLING_FF, PH_FF});   // couplingF.cuh:103
   if (h && g.n_har >= 3) a.push_back({GGB_COUPLING_FP, PH_FP});   // couplingP.cuh:148
   if (h && g.n_har >= 3) a.push_back({GGB_COUPLING_D, PH_D});     // couplingD.cuh:103 (v_2 = 0 without Hartree)
@@ -203,7 +210,8 @@ static void build_chain(GroupHost& g, const std::vector<Act>& seq, int half, int
   const size_t per_m = (size_t)n_l * ldS, per_mat = per_m * n_m;
   const int k = (int)seq.size();
   ch.n_ops = k + 1;
-  const bool s_on = g.n_har >= 3 && g.use_hartree == 1 && g.target_id > 0;  // couplingS.cuh:18,49
+  // couplingS.cuh:18,49; the theta form carries the S terms in its one phase
+  const bool s_on = !g.theta && g.n_har >= 3 && g.use_hartree == 1 && g.target_id > 0;
   ch.pre_s = (half == 1) && s_on;
   ch.post_s = (half == 0) && s_on;
   for (int o = 0; o <= k; ++o) {
@@ -290,6 +298,7 @@ static int prepare(ggb_ctx* ctx) {
     a.n_runs = (int)g.runs.size();
     a.hartree_on = (g.use_hartree == 1 && g.target_id > 0);
     a.p_hartree = (g.use_hartree == 1 && g.n_har > 1 && g.target_id > 0);
+    a.theta = g.theta;
     a.n_den = a.hartree_on ? std::min(g.n_har, N_DEN) : 0;
     a.per_l = ctx->dims.per_l;
     a.dt = g.dt;
@@ -420,12 +429,16 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     if (r.d.group < 0 || r.d.group >= dims->n_groups || r.d.n_orb <= 0 || r.d.n_har < 0 || !(r.d.dt > 0.0))
       return bad(GGB_ERR_ARG, "run dims");
     GroupHost& g = ctx->groups[r.d.group];
+    const int theta = (r.d.flags & GGB_RUN_THETA) ? 1 : 0;
+    if (theta && dims->precision == GGB_SPLIT_BF16) return bad(GGB_ERR_ARG, "theta form with split_bf16");
+    if (theta && r.d.n_har > N_DEN) return bad(GGB_ERR_ARG, "theta form: n_har > 4");
     if (!g.runs.empty()) {
       if (g.n_har != r.d.n_har || g.use_hartree != r.d.use_hartree || (g.target_id > 0) != (r.d.target_id > 0) ||
-          g.dt != r.d.dt)
-        return bad(GGB_ERR_ARG, "runs of a group must share n_har, use_hartree, targetID>0 and dt");
+          g.dt != r.d.dt || g.theta != theta)
+        return bad(GGB_ERR_ARG, "runs of a group must share n_har, use_hartree, targetID>0, dt and the theta flag");
     } else {
       g.n_har = r.d.n_har; g.use_hartree = r.d.use_hartree; g.target_id = r.d.target_id; g.dt = r.d.dt;
+      g.theta = theta;
     }
     r.col0 = g.n_cols;
     g.n_cols += r.d.n_orb;
@@ -581,20 +594,22 @@ int ggb_step(ggb_ctx* ctx, int n_steps, void* stream) {
   if (!ctx->graph_exec) {
     // capture once, on the first call, so that later calls only replay
     if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-    cudaGraph_t graph;
-    CK(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    const int rc_cap = launch_steps(ctx, ctx->cap_stream, G);
-    CK(cudaStreamEndCapture(ctx->cap_stream, &graph));
-    if (rc_cap) {
+    for (int k = 0; k < 2; ++k) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+      const int rc_cap = launch_steps(ctx, ctx->cap_stream, k == 0 ? G : 1);
+      CK(cudaStreamEndCapture(ctx->cap_stream, &graph));
+      if (rc_cap) {
+        cudaGraphDestroy(graph);
+        return rc_cap;
+      }
+      CK(cudaGraphInstantiate(k == 0 ? &ctx->graph_exec : &ctx->graph1_exec, graph, 0));
       cudaGraphDestroy(graph);
-      return rc_cap;
     }
-    CK(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
-    cudaGraphDestroy(graph);
   }
   if (n_steps == 0) return GGB_OK;
   for (int i = 0; i + G <= n_steps; i += G) CK(cudaGraphLaunch(ctx->graph_exec, s));
-  if ((rc = launch_steps(ctx, s, n_steps % G))) return rc;
+  for (int i = 0; i < n_steps % G; ++i) CK(cudaGraphLaunch(ctx->graph1_exec, s));
   CK(cudaGetLastError());
   return GGB_OK;
 }
@@ -715,6 +730,7 @@ void ggb_destroy(ggb_ctx* ctx) {
   if (!ctx) return;
   cudaDeviceSynchronize();
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph1_exec) cudaGraphExecDestroy(ctx->graph1_exec);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   for (cudaStream_t gs : ctx->group_streams) cudaStreamDestroy(gs);
   for (cudaEvent_t e : ctx->group_done) cudaEventDestroy(e);

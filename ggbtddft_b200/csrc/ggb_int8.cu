@@ -543,7 +543,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       sb = run.v[rc] - run.v0[rc] + run.vexc[rc] - run.vexc0[rc];
     }
     pbase[0][p] = rr;
-    pbase[1][p] = (g.p_hartree ? (rr * E + v1) : (rr * E)) * hdt;
+    pbase[1][p] = ((g.p_hartree || g.theta) ? (rr * E + v1) : (rr * E)) * hdt;
     pbase[2][p] = v2 * hdt;
     pbase[3][p] = v3 * hdt;
     pbase[4][p] = sb * hdt;
@@ -702,6 +702,9 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
       const double dj = (op.phase != PH_NONE && j >= m && j < n_l) ? Dv[j] : 0.0;
       const int pb = op.phase == PH_P ? 1 : op.phase == PH_D ? 2 : 3;
+      // the theta form: angle = pbase1 x_j + pbase2 P_2(x_j) + pbase3 P_3(x_j) + pbase4 (all x dt/2)
+      const bool th = op.phase == PH_THETA && j >= m && j < n_l;
+      const double p2j = th ? legendre_p2(dj) : 0.0, p3j = th ? legendre_p3(dj) : 0.0;
       const bool post_s = last && !SECOND_HALF && ch.post_s && j < n_l;
       const double pj = post_s ? pco[j] : 0.0;
       const double sj = pow2i(-t.sexp[((size_t)op.mat * g.n_m + m) * t.rows + j]);   // S^T row scale
@@ -738,7 +741,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int p = p0 + u;
-          if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
+          if (th) v[u] = rotd(v[u], pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p]);
+          else if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
           if (post_s) v[u] = rotd(v[u], pbase[4][p] + pj * pbase[2][p]);
           if (!last) {
             if (j < lk) {

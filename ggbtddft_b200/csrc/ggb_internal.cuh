@@ -29,7 +29,15 @@ constexpr unsigned ST_NAN = 1u;
 constexpr unsigned ST_STEP_OVERFLOW = 2u;
 constexpr unsigned ST_NORM_GROWTH = 4u;
 
-enum PhaseKind { PH_NONE = 0, PH_P = 1, PH_FP = 2, PH_D = 3, PH_FF = 4 };
+// PH_THETA: the theta form's one phase at the P coupling's nodes x_j,
+//   (r E + v_1) x_j + v_2 P_2(x_j) + v_3 P_3(x_j) + (v_0 - v_0(t=0)) + (vxc - vxc(t=0))
+enum PhaseKind { PH_NONE = 0, PH_P = 1, PH_FP = 2, PH_D = 3, PH_FF = 4, PH_THETA = 5 };
+constexpr int RUN_FLAG_PW92 = 1;
+constexpr int RUN_FLAG_THETA = 2;
+
+// P_2 and P_3 of the theta phase
+__host__ __device__ __forceinline__ double legendre_p2(double x) { return 0.5 * (3.0 * x * x - 1.0); }
+__host__ __device__ __forceinline__ double legendre_p3(double x) { return 0.5 * x * (5.0 * x * x - 3.0); }
 enum Coef { CF_CU = 0, CF_CD = 1, CF_P = 2, CF_QU = 3, CF_QD = 4, CF_P3 = 5, CF_F3 = 6, COEF_N = 7 };
 
 struct ChainOp {
@@ -67,6 +75,7 @@ struct RunDev {
 
 struct GroupArgs {
   int n_r, n_l, n_m, n_cols, n_tiles, ldS, n_runs;
+  int theta;        // theta form (GGB_RUN_THETA): one phase per half-step at the P nodes
   int hartree_on;   // USE_HARTREE == 1 && targetID > 0
   int p_hartree;    // P phase carries v_1 (USE_HARTREE && N_har > 1 && targetID > 0)
   int n_den;        // multipoles computed: min(N_har, 4) when hartree_on, else 0

@@ -124,7 +124,13 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
         if (j < n_l) {
           double2 y = acc[q];
           // phase in the eigenbasis (couplingP.cuh:61-106 and twins)
-          if (op.phase != PH_NONE && j >= m) {
+          if (op.phase == PH_THETA && j >= m) {
+            // the theta form: the whole angular potential at node x_j
+            const double xj = Dv[j];
+            double eta = (rr * E + v1) * xj + v2 * legendre_p2(xj) + v3 * legendre_p3(xj) + sbase;
+            eta *= hdt;
+            y = cmul_conj_phase(y, eta);
+          } else if (op.phase != PH_NONE && j >= m) {
             double eta = base;
             eta *= hdt * Dv[j];
             y = cmul_conj_phase(y, eta);
@@ -421,7 +427,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
   // exchange (block L = 0, or the observables block when Hartree is off)
   const bool xc_block = (g.n_den > 0) ? (role == 0) : obs_block;
   if (xc_block) {
-    const bool pw92 = (run.flags & 1) != 0;
+    const bool pw92 = (run.flags & RUN_FLAG_PW92) != 0;
     for (int q = tid; q < n_r; q += FIN_THREADS) {
       double rho0 = 0.0;
       if (g.n_den > 0) rho0 = fsm[q];

@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libggbtddft.so")
 PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_tf32": 2, "split_int8": 3}
 COUPLING_IDS = {"P": 0, "FP": 1, "D": 2, "FF": 3}
 RUN_XC_PW92 = 1
+RUN_THETA = 2
 
 
 class GGBError(RuntimeError):
@@ -52,7 +53,7 @@ _lib = None
 EXPORTS = ("ggb_create", "ggb_set_grid", "ggb_set_radial_propagators", "ggb_set_angular", "ggb_set_orbitals",
            "ggb_set_field", "ggb_step", "ggb_get_step", "ggb_get_observables", "ggb_get_orbitals",
            "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase",
-           "ggb_set_tuning", "ggb_observables_noalloc")
+           "ggb_set_tuning", "ggb_observables_noalloc", "ggb_measure_peaks")
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -84,6 +85,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_destroy": ([P], None),
         "ggb_version": ([], ctypes.c_char_p),
         "ggb_observables_noalloc": ([P, P, P, I_, I_, I_, P, P, P, P], I_),
+        "ggb_measure_peaks": ([ctypes.POINTER(D), ctypes.POINTER(D), P], I_),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -99,6 +101,16 @@ def _ptr(a: Optional[np.ndarray]):
 
 def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
+
+
+def measure_peaks(stream: Optional[int] = None) -> Dict[str, float]:
+    """FP64 FMA (TFLOP/s) and tcgen05 int8 (TOP/s) peaks of the current GPU (ggb_measure_peaks)."""
+    lib = load_library()
+    f, i = ctypes.c_double(), ctypes.c_double()
+    rc = lib.ggb_measure_peaks(ctypes.byref(f), ctypes.byref(i), ctypes.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise GGBError(f"ggb_measure_peaks failed: {rc}")
+    return dict(fp64_tflops=f.value, int8_tops=i.value)
 
 
 def group_runs(runs: Sequence[RunInputs]) -> List[List[int]]:
@@ -146,7 +158,8 @@ class TimePropagation:
         rd = (_RunDesc * len(self.runs))()
         for i, r in enumerate(self.runs):
             rd[i] = _RunDesc(run_group[i], r.n_orb, r.n_har, r.use_hartree, r.target_id,
-                             RUN_XC_PW92 if r.xc_correlation else 0, r.dt)
+                             (RUN_XC_PW92 if r.xc_correlation else 0) |
+                             (RUN_THETA if getattr(r, "angular", "reference") == "theta" else 0), r.dt)
         dims = _Dims(len(self.groups), len(self.runs), PRECISIONS[precision], self.n_t, 1 if per_l else 0)
         ctx = ctypes.c_void_p()
         self._check(self.lib.ggb_create(ctypes.byref(dims), gd, rd, ctypes.byref(ctx)), None)

@@ -43,6 +43,7 @@ class RunInputs:
     xc_correlation: bool = False
     name: str = ""
     omega0: float = 0.057
+    angular: str = "reference"     # "reference": the FF/FP/D/P/S chain; "theta": one phase at the P nodes
 
     @property
     def n_r(self) -> int:
@@ -78,7 +79,7 @@ def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.
               mask_width: Optional[float] = None, n_har: int = 4, use_hartree: int = 1,
               target_id: int = 0, xc_correlation: bool = False, name: str = "",
               omega0: float = 0.057, device: Optional[str] = None,
-              W: Optional[np.ndarray] = None) -> RunInputs:
+              W: Optional[np.ndarray] = None, angular: str = "reference") -> RunInputs:
     """Assemble one run.
 
     absorber = "cap":  the reference's Manolopoulos CAP starting at ``cap_r_mask``, entering the
@@ -116,7 +117,7 @@ def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.
         occ=np.array([o.occ for o in gs.orbitals], dtype=np.int32),
         rho_frozen=gs.rho_frozen.copy(), E=np.ascontiguousarray(E, dtype=np.float64),
         n_har=n_har, use_hartree=use_hartree, target_id=target_id,
-        xc_correlation=xc_correlation, name=name, omega0=omega0)
+        xc_correlation=xc_correlation, name=name, omega0=omega0, angular=angular)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -127,12 +128,14 @@ def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H",
                    r_mask: float = 30.0, zeta_ref: float = 1.0, dt_as: float = 20.0,
                    intensity: float = 2e14, omega0: float = 0.057, cycles: float = 1.0,
                    cep: float = 0.5 * math.pi, n_har: int = 4, use_hartree: int = 1,
-                   seed: int = 0, perturb: float = 0.0) -> RunInputs:
+                   seed: int = 0, perturb: float = 0.0, device: Optional[str] = None) -> RunInputs:
     """A run built the way the reference's init.py builds one (CAP twice, super-Gaussian, CN).
 
     atom "H": hydrogen-like 1s, targetID 0 (no Hartree/XC in the loop).
     atom "Ne3": a 3-orbital LDA atom (1s, 2p0, 2p1; occ 2,2,4; targetID 2) so that every
     coupling (P, FP, D, FF, S), the Hartree multipoles and the exchange potential are active.
+    atom "Ar9": argon's nine orbitals (Z = 18, LDA), targetID 5, all couplings active: the size of
+    the argon workloads on the reference's own code path.
     ``perturb`` mixes seeded random noise into the initial orbitals (then renormalises) so that
     the parity tests also exercise components that vanish for exact eigenstates.
     """
@@ -146,6 +149,9 @@ def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H",
         orbs = [I.Orbital(1, 0, 0, 2), I.Orbital(2, 1, 0, 2), I.Orbital(2, 1, 1, 4)]
         gs = I.ground_state(grid, 8.0, orbs, interacting=True, iterations=60)
         target_id = 2
+    elif atom == "Ar9":
+        gs = I.ground_state(grid, 18.0, I.ORBITALS_AR, interacting=True, device=device)
+        target_id = 5
     else:
         raise ValueError(atom)
     if perturb:
@@ -159,7 +165,7 @@ def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H",
     E = I.field_super_gaussian(t, e0, omega0, tau0, cep)
     return build_run(grid, n_l, dt, gs, E, absorber="cap", cap_r_mask=r_mask, cap_passes=2,
                      n_har=n_har, use_hartree=use_hartree, target_id=target_id,
-                     name=f"{atom}-N{n_r}-L{n_l}", omega0=omega0)
+                     name=f"{atom}-N{n_r}-L{n_l}", omega0=omega0, device=device)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -201,7 +207,7 @@ ATOMS = {
 def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser: LaserSpec,
                  mask_width: float, zeta: float = 0.5, n_steps: Optional[int] = None,
                  device: Optional[str] = None, gs_cache: Optional[dict] = None,
-                 W: Optional[np.ndarray] = None) -> RunInputs:
+                 W: Optional[np.ndarray] = None, angular: str = "reference") -> RunInputs:
     """One of the benchmark configurations: sin^2 pulse, cos^(1/8) mask, Z = true nuclear charge.
 
     Hartree/XC runs use the reference's multipole treatment (L <= 3, N_har = 4) with Slater
@@ -223,7 +229,8 @@ def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser
     return build_run(grid, l_max + 1, dt, gs, E, absorber="mask", mask_width=mask_width,
                      n_har=4 if spec.interacting else 2, use_hartree=1 if spec.interacting else 0,
                      target_id=target, xc_correlation=spec.correlation,
-                     name=f"{atom}-N{n_r}-L{l_max}", omega0=laser.omega, device=device, W=W)
+                     name=f"{atom}-N{n_r}-L{l_max}", omega0=laser.omega, device=device, W=W,
+                     angular=angular)
 
 
 def config_hydrogen(n_steps=None, device=None) -> RunInputs:
@@ -267,20 +274,39 @@ def quiver_radius(laser: LaserSpec) -> float:
     return laser.e0 / laser.omega ** 2
 
 
-def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = None, device=None,
-                   ladder: Sequence[GridRung] = ARGON_LADDER, only=None) -> List[RunInputs]:
+@dataclasses.dataclass
+class EnsembleDraws:
+    """The seeded laser parameters of an ensemble and the ladder rung (grid) of each run."""
+    atoms: List[str]
+    intensity: np.ndarray
+    wavelength_nm: np.ndarray
+    cep: np.ndarray
+    rung: np.ndarray
+    cycles: float
+    dt: float
+    ladder: Sequence[GridRung]
+
+    def grid_groups(self) -> Dict[tuple, List[int]]:
+        """{(rung, atom): run indices}: the runs that share a grid and radial propagators (one grid
+        group of the batched step), in ladder order."""
+        out: Dict[tuple, List[int]] = {}
+        for i, k in enumerate(self.rung):
+            out.setdefault((int(k), self.atoms[i]), []).append(i)
+        return dict(sorted(out.items()))
+
+
+def argon_draws(n_runs: int = 64, seed: int = 0, ladder: Sequence[GridRung] = ARGON_LADDER) -> EnsembleDraws:
     """Argon LDA in-situ focal scan: I ~ U[0.8, 2]e14 W/cm^2, lambda ~ U[800, 1300] nm, 10-cycle sin^2,
     dt = 0.02, 9 orbitals; each run goes on the ladder rung indexed by its wavelength
     (longer wavelength -> larger excursion and higher cutoff -> larger grid and l_max)."""
     rng = np.random.default_rng(seed)
     I0 = rng.uniform(0.8e14, 2.0e14, n_runs)
     lam = rng.uniform(800.0, 1300.0, n_runs)
-    return _ensemble("Ar", I0, lam, np.zeros(n_runs), 10.0, 0.02, n_steps, device, ladder,
-                     lambda l: min(len(ladder) - 1, int((l - 800.0) / 100.0)), only=only)
+    rung = np.array([min(len(ladder) - 1, int((l - 800.0) / 100.0)) for l in lam])
+    return EnsembleDraws(["Ar"] * n_runs, I0, lam, np.zeros(n_runs), rung, 10.0, 0.02, ladder)
 
 
-def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None, device=None,
-                 ladder: Sequence[GridRung] = HHE_LADDER, only=None) -> List[RunInputs]:
+def hhe_draws(n_runs: int = 256, seed: int = 0, ladder: Sequence[GridRung] = HHE_LADDER) -> EnsembleDraws:
     """H/He-like scan: I log-uniform in [0.5, 3]e14, CEP ~ U[0, 2 pi), lambda ~ U[800, 1800] nm,
     6-cycle sin^2, dt = 0.03; atoms alternate H / He; the rung is the smallest whose r_max covers
     3 quiver radii plus the absorber."""
@@ -296,21 +322,33 @@ def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None
                 return k
         return len(ladder) - 1
     atoms = ["H" if i % 2 == 0 else "He" for i in range(n_runs)]
-    return _ensemble(atoms, I0, lam, cep, 6.0, 0.03, n_steps, device, ladder, None, rung_of_run=rung, only=only)
+    return EnsembleDraws(atoms, I0, lam, cep, np.array([rung(i) for i in range(n_runs)]), 6.0, 0.03, ladder)
 
 
-def _ensemble(atom, I0, lam, cep, cycles, dt, n_steps, device, ladder, rung_of_lambda, rung_of_run=None,
-              only=None):
+def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = None, device=None,
+                   ladder: Sequence[GridRung] = ARGON_LADDER, only=None) -> List[RunInputs]:
+    """The runs of ``argon_draws``."""
+    return _ensemble(argon_draws(n_runs, seed, ladder), n_steps, device, only=only)
+
+
+def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None, device=None,
+                 ladder: Sequence[GridRung] = HHE_LADDER, only=None) -> List[RunInputs]:
+    """The runs of ``hhe_draws``."""
+    return _ensemble(hhe_draws(n_runs, seed, ladder), n_steps, device, only=only)
+
+
+def _ensemble(dr: EnsembleDraws, n_steps, device, only=None):
     """The runs of an ensemble from its drawn parameters; ``only`` = indices of the runs to build
     (the draws are made for the whole ensemble first, so a selected run equals its twin in the full
     ensemble)."""
-    n_runs = len(I0)
+    n_runs = len(dr.intensity)
+    I0, lam, cep, cycles, dt, ladder = dr.intensity, dr.wavelength_nm, dr.cep, dr.cycles, dr.dt, dr.ladder
     runs: List[RunInputs] = []
     gs_cache: dict = {}
     w_cache: dict = {}
     for i in (range(n_runs) if only is None else only):
-        a = atom[i] if isinstance(atom, list) else atom
-        k = rung_of_run(i) if rung_of_run is not None else rung_of_lambda(lam[i])
+        a = dr.atoms[i]
+        k = int(dr.rung[i])
         g = ladder[k]
         laser = LaserSpec(float(I0[i]), float(lam[i]), cycles, float(cep[i]))
         key = (a, g.n_r, g.r_max, g.l_max)

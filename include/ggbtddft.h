@@ -44,7 +44,13 @@ enum { GGB_COUPLING_P = 0, GGB_COUPLING_FP = 1, GGB_COUPLING_D = 2, GGB_COUPLING
 
 /* run flags */
 enum {
-  GGB_RUN_XC_PW92 = 1   /* add PW92 correlation to the TD exchange potential (not in the reference) */
+  GGB_RUN_XC_PW92 = 1,  /* add PW92 correlation to the TD exchange potential (not in the reference) */
+  GGB_RUN_THETA = 2     /* theta form (not in the reference): each angular half-step is one diagonal
+                           phase at the Gauss nodes of the P coupling (its eigenbasis, the V/D of
+                           coupling P), exp(-i dt/2 [r E x_j + sum_{L=1}^{3} v_L(r) P_L(x_j) + dv_0(r)
+                           + dv_xc(r)]), instead of the reference's FF/FP/D/P/S chain: two products
+                           per half-step; multipoles L < min(n_har, 4).  Runs of a group share it;
+                           the split_int8 and FP64 forms only. */
 };
 
 /* error codes */
@@ -113,7 +119,8 @@ int ggb_set_field(ggb_ctx* ctx, int run, const double* E, int n_t);
 
 /* Advance every run by n_steps steps, asynchronously on `stream` (a cudaStream_t).
    The first call after ggb_set_orbitals computes the initial potentials
-   (h_timePropagation.cuh:47-57).  Replays one captured CUDA graph per chunk of steps. */
+   (h_timePropagation.cuh:47-57).  Every step runs from a captured CUDA graph: a 32-step graph
+   replayed n_steps / 32 times, then a 1-step graph n_steps % 32 times. */
 int ggb_step(ggb_ctx* ctx, int n_steps, void* stream);
 
 /* Profiling hook: launch one phase of the step for every group on `stream`
@@ -173,6 +180,13 @@ void ggb_destroy(ggb_ctx* ctx);
    first call before any stream capture. */
 int ggb_observables_noalloc(const double* x, const double* r, const int* m, int n_l, int n_orb, int n_r,
                             double* dip, double* acc, double* norm, void* stream);
+
+/* Peak throughput of the current GPU, measured with the library's own microbenchmark kernels (no
+   device allocation): FP64 FMA on the CUDA cores in TFLOP/s, and tcgen05.mma kind::i8 (M 128, N 256,
+   K 32, int32 accumulation in tensor memory) in TOP/s; either pointer may be NULL.  Synchronous on
+   `stream`, a few tens of milliseconds.  These are the denominators of the roofline fractions of the
+   FP64 and int8 forms.  No counterpart in the reference. */
+int ggb_measure_peaks(double* fp64_tflops, double* int8_tops, void* stream);
 
 /* Library version string. */
 const char* ggb_version(void);

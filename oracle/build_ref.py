@@ -13,6 +13,13 @@ Run the binary on a GPU with ``cd oracle/_ref/<case>/run && ../ggb_ref``; it rea
 ``./workingData`` and writes ``../output/<date>/<idx>/...``.  ``tests/golden/make_ref_fixtures.py``
 turns those outputs into the committed golden fixtures.
 
+Timed cases (``TIMED_CASES``) are built the same way, with one addition in their generated
+params.cuh: the reference's ``h_timePropagation`` (h_timePropagation.cuh:32-114) is included under
+another name and wrapped by a function of that name that brackets it with cudaEvents and prints
+``GGB_REF_TIMING scan=<s> steps=<N_t> ms=<t>`` (the reference's sources are not modified; main.cu
+calls the wrapper).  Their workingData is large (W alone is N_l N_r^2 16 bytes), so it is not
+written here: ``oracle/time_ref.py`` writes it on the GPU machine and runs the binary.
+
 The reference's GSL includes are unused (main.cu:15-18); empty stub headers satisfy them.
 ``-arch=sm_30`` of ``src/compile:1`` is not supported by CUDA 12.9, so the build targets sm_100a.
 Only sizes that are multiples of 32 are valid for the reference (its launch grids truncate).
@@ -41,6 +48,47 @@ CASES = {
 }
 
 
+# timed case name -> reference_like() keyword arguments (sizes multiples of 32, as the reference needs)
+TIMED_CASES = {
+    "ar9_608": dict(n_r=608, n_l=96, n_t=200, atom="Ar9", r_mask=200.0, zeta_ref=2.0 * 0.5 / 300.0,
+                    dt_as=0.02 / 0.041341373335182,
+                    intensity=1.4e14, omega0=0.057, cycles=2.0),
+}
+
+TIMING_WRAPPER = """
+// Timing wrapper of this build only (not part of the reference): the reference's h_timePropagation
+// is included above under the name h_timePropagation_untimed and bracketed here by cudaEvents.
+void h_timePropagation (ksoSetTDStruct ksoSetTD, hartreeStruct hartree, propagatorsStruct propagators,
+                        meshStruct mesh, observableStruct observables, tempStruct temp, handleStruct handles,
+                        int scandx)
+{
+	cudaEvent_t ggb_e0, ggb_e1;
+	float ggb_ms = 0.0f;
+	cudaEventCreate(&ggb_e0);
+	cudaEventCreate(&ggb_e1);
+	cudaDeviceSynchronize();
+	cudaEventRecord(ggb_e0, 0);
+	h_timePropagation_untimed(ksoSetTD, hartree, propagators, mesh, observables, temp, handles, scandx);
+	cudaEventRecord(ggb_e1, 0);
+	cudaEventSynchronize(ggb_e1);
+	cudaEventElapsedTime(&ggb_ms, ggb_e0, ggb_e1);
+	printf("GGB_REF_TIMING scan=%d steps=%d ms=%.4f\\n", scandx, N_t, ggb_ms);
+	cudaEventDestroy(ggb_e0);
+	cudaEventDestroy(ggb_e1);
+}
+"""
+
+
+def add_timing_wrapper(params_path: str) -> None:
+    """Rename the reference's h_timePropagation at its include and append the timed wrapper."""
+    inc = '#include "./subFunctions/timePropagation/h_timePropagation.cuh"'
+    s = open(params_path).read()
+    assert s.count(inc) == 1
+    s = s.replace(inc, "#define h_timePropagation h_timePropagation_untimed\n" + inc + "\n#undef h_timePropagation")
+    with open(params_path, "w") as f:
+        f.write(s + TIMING_WRAPPER)
+
+
 def field_params(kw):
     import math
     from ggbtddft_b200 import inputs as I
@@ -49,15 +97,18 @@ def field_params(kw):
                 tau0=kw.get("cycles", 1.0) * 2.0 * math.pi / omega0, cep0=kw.get("cep", 0.5 * math.pi))
 
 
-def build_case(name: str, kw: dict, nvcc: str = "nvcc") -> str:
+def build_case(name: str, kw: dict, nvcc: str = "nvcc", timed: bool = False) -> str:
     from ggbtddft_b200 import problems as P, workingdata as WD
     d = os.path.join(OUT, name)
     os.makedirs(os.path.join(d, "run"), exist_ok=True)
     run = P.reference_like(**kw)
     fp = field_params(kw)
-    Z = 1.0 if kw.get("atom", "H") == "H" else 8.0
-    WD.write_working_data(run, os.path.join(d, "run"))
+    Z = {"H": 1.0, "Ne3": 8.0, "Ar9": 18.0}[kw.get("atom", "H")]
+    if not timed:
+        WD.write_working_data(run, os.path.join(d, "run"))
     WD.write_params_cuh(run, os.path.join(d, "params.cuh"), sim_date=SIM_DATE, sim_index=SIM_INDEX, Z=Z, **fp)
+    if timed:
+        add_timing_wrapper(os.path.join(d, "params.cuh"))
     WD.output_dirs(os.path.join(d, "output"), SIM_DATE, SIM_INDEX, 1, run.n_orb)
     for link, target in (("main.cu", f"{REF_SRC}/main.cu"), ("subFunctions", f"{REF_SRC}/subFunctions")):
         p = os.path.join(d, link)
@@ -87,9 +138,12 @@ def main(argv=None):
     if not os.path.isdir(REF_SRC):
         print("reference sources not present; nothing to build")
         return 0
-    names = (argv or sys.argv[1:]) or list(CASES)
+    names = (argv or sys.argv[1:]) or list(CASES) + list(TIMED_CASES)
     for n in names:
-        print("built", build_case(n, CASES[n]))
+        if n in TIMED_CASES:
+            print("built", build_case(n, TIMED_CASES[n], timed=True))
+        else:
+            print("built", build_case(n, CASES[n]))
     return 0
 
 

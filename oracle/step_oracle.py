@@ -15,11 +15,16 @@ the checker.  It restates, operation by operation and in the same order, the ref
 * ``src/subFunctions/timePropagation/observables/dipoleMoment.cuh``, ``dipoleAcceleration.cuh``
 
 Parity pin: this restatement is checked against the reference binary (``main.cu`` built for
-sm_100a from the reference's own sources by ``oracle/build_ref.sh``) on identical workingData;
+sm_100a from the reference's own sources by ``oracle/build_ref.py``) on identical workingData;
 the resulting dipole files are committed as golden fixtures under ``tests/golden/``.
 
 Options beyond the reference (off by default, so the default reproduces the reference):
-``xc_correlation`` (adds PW92 correlation to the TD exchange potential) and the ``norm`` output.  The reference's truncation of every pointwise launch to
+``xc_correlation`` (adds PW92 correlation to the TD exchange potential), the ``norm`` output, and
+``angular = "theta"``: the angular half-step as one diagonal phase at the Gauss nodes of the dipole
+coupling (the eigenbasis of the reference's P coupling, couplingP.cuh:1-125), holding the laser term
+and the Hartree potential of the multipoles L = 0 .. n_har - 1 (n_har up to 2 l_max + 1) with the
+exchange(-correlation) change -- see ``OracleState.step_theta``.  With n_har <= 4 its multipoles are
+the reference's l-space sums; beyond, exact Gauss-Legendre quadratures of the density on 2 N_l nodes.  The reference's truncation of every pointwise launch to
 multiples of 32 (e.g. ``couplingP.cuh:117``) is NOT reproduced: full ranges are used, which
 equals the reference whenever N_r and N_l are multiples of 32.
 """
@@ -121,6 +126,7 @@ class OracleProblem:
     target_id: int = 0
     # options beyond the reference (defaults reproduce it)
     xc_correlation: bool = False
+    angular: str = "reference"      # "reference" | "theta"
 
     @property
     def n_r(self):
@@ -168,6 +174,53 @@ def _coupling(x, prob: OracleProblem, name: str, eta_r: Optional[np.ndarray]):
     return out
 
 
+def legendre_table(x: np.ndarray, n: int) -> np.ndarray:
+    """P_L(x) for L = 0 .. n-1 (rows), by the three-term recurrence (L+1) P_{L+1} = (2L+1) x P_L - L P_{L-1}."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.zeros((max(n, 1),) + x.shape)
+    out[0] = 1.0
+    if n > 1:
+        out[1] = x
+    for L in range(1, n - 1):
+        out[L + 1] = ((2.0 * L + 1.0) * x * out[L] - L * out[L - 1]) / (L + 1.0)
+    return out[:n]
+
+
+def assoc_legendre_normalised(x: np.ndarray, n_l: int, m: int) -> np.ndarray:
+    """Theta_l(x) for l = 0 .. n_l-1 (rows; zero for l < m): the associated Legendre functions of order
+    m normalised to int_{-1}^{1} Theta_l^2 dx = 1, with the signs fixed by the recurrence of the
+    dipole coupling, x Theta_l = c_u(l, m) Theta_{l+1} + c_d(l, m) Theta_{l-1} (angularCoefficients.cuh),
+    so that an orbital's coefficients x_l are the coefficients of sum_l x_l Theta_l(cos theta)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.zeros((n_l,) + x.shape)
+    if m >= n_l:
+        return out
+    # Theta_m = C (1 - x^2)^(m/2), C^2 = (2m+1)! / (2^(2m+1) (m!)^2), built as a product to stay finite
+    c2 = 0.5
+    for k in range(1, m + 1):
+        c2 *= (2.0 * k + 1.0) * (2.0 * k) / (4.0 * k * k)
+    out[m] = np.sqrt(c2) * np.power(1.0 - x * x, 0.5 * m)
+    if m + 1 < n_l:
+        out[m + 1] = x * out[m] / c_u(m, m)
+    for l in range(m + 1, n_l - 1):
+        out[l + 1] = (x * out[l] - c_d(l, m) * out[l - 1]) / c_u(l, m)
+    return out
+
+
+def hartree_multipoles_scaled(r: np.ndarray, dens: np.ndarray) -> np.ndarray:
+    """v_L(r_a) = sum_b rho_L(b) r_<^L / r_>^(L+1) for every row L of ``dens``, evaluated as
+    sum_b rho_L(b) (r_< / r_>)^L / r_> so that no power of r over- or underflows for large L
+    (the reference's direct sum, h_calculateHartreePotential.cuh:22-51, extended past L = 3)."""
+    rmax = np.maximum(r[:, None], r[None, :])
+    ratio = np.minimum(r[:, None], r[None, :]) / rmax
+    k = 1.0 / rmax
+    v = np.zeros_like(dens)
+    for L in range(dens.shape[0]):
+        v[L] = k @ dens[L]
+        k = k * ratio
+    return v
+
+
 class OracleState:
     def __init__(self, prob: OracleProblem):
         self.p = prob
@@ -186,6 +239,19 @@ class OracleState:
         self._cu = np.stack([c_u(l_idx, mm) for mm in prob.m])     # [kso, l]
         self._cd = np.stack([c_d(l_idx, mm) for mm in prob.m])
         self._p = np.stack([p_lm(l_idx, mm) for mm in prob.m])
+        self.theta = prob.angular == "theta"
+        if self.theta:
+            # Legendre values at each m's Gauss nodes (the P coupling's eigenvalues, j >= m):
+            # pl[m][L][j] = P_L(D_P[m][j])
+            n_m = int(np.max(prob.m)) + 1
+            self.pl = np.stack([legendre_table(prob.D["P"][mm], max(prob.n_har, 1)) for mm in range(n_m)])
+            self.htab = np.zeros((n_m, prob.n_l, n_r))     # H_m(r, j) as [m][j][r]
+            if prob.n_har > 4:
+                # exact multipoles: Gauss-Legendre quadrature on 2 N_l nodes (degree 4 l_max + 3 >= the
+                # l + l' + L <= 4 l_max of every term)
+                xq, wq = np.polynomial.legendre.leggauss(2 * prob.n_l)
+                self.fine_t = np.stack([assoc_legendre_normalised(xq, prob.n_l, mm).T for mm in range(n_m)])
+                self.fine_pw = legendre_table(xq, prob.n_har) * wq[None, :]      # [L][q]
 
     # ----- potentials -----
     def density_multipoles(self, x):
@@ -329,8 +395,66 @@ class OracleState:
             vx = vx + _pw92(n)
         return vx
 
+    # ----- theta mode -----
+    def nodal_density(self, x):
+        """rho_m(r, j) = sum over the orbitals with m of occ |(V_P,m^T x)_j(r)|^2: the density at the
+        Gauss nodes of each m ([n_m][N_l][N_r]; rows j < m are zero)."""
+        p = self.p
+        n_m = self.pl.shape[0]
+        out = np.zeros((n_m, p.n_l, p.n_r))
+        V = p.V["P"]
+        for k in range(p.n_kso):
+            m = int(p.m[k])
+            y = V[m][m:, m:].T @ x[m:, k, :]
+            out[m, m:] += float(p.occ[k]) * (y.real ** 2 + y.imag ** 2)
+        return out
+
+    def theta_multipoles(self, x):
+        """rho_L(r) = sum_m sum_j rho_m(r, j) P_L(x_j^m), L = 0 .. n_har-1: the quadrature of each m's
+        density over its own N_l - m nodes.  Exact for L <= 1 only (for larger L the top multipoles
+        alias by several per cent): a check, not what the theta form uses."""
+        nd = self.nodal_density(x)
+        return np.einsum("mlj,mjr->lr", self.pl, nd)
+
+    def fine_multipoles(self, x):
+        """rho_L(r) = sum_k occ_k int |sum_l x_l Theta_l^(m_k)(t)|^2 P_L(t) dt for L = 0 .. n_har-1, by
+        Gauss-Legendre quadrature on 2 N_l nodes, exact for every L <= 2 l_max."""
+        p = self.p
+        rho_q = np.zeros((self.fine_pw.shape[1], p.n_r))
+        for k in range(p.n_kso):
+            f = self.fine_t[int(p.m[k])] @ x[:, k, :]            # [q][r]
+            rho_q += float(p.occ[k]) * (f.real ** 2 + f.imag ** 2)
+        return self.fine_pw @ rho_q
+
+    def theta_density(self, x):
+        """The theta form's multipoles: the reference's l-space sums for n_har <= 4, else exact."""
+        if self.p.n_har <= 4:
+            return self.density_multipoles(x)
+        return self.fine_multipoles(x)
+
+    def theta_hartree(self, dens):
+        if self.p.n_har <= 4:
+            return self.hartree_from_density(dens)
+        return hartree_multipoles_scaled(self.p.r, dens)
+
+    def theta_table(self):
+        """H_m(r, j) = sum_{L>=1} v_L(r) P_L(x_j^m) + (v_0 - v_0^(0)) + (vxc - vxc^(0)): the potential
+        change since t = 0 at the nodes (the ground state's spherical potential is inside W)."""
+        s_r = self.v[0] - self.v0 + self.vexc - self.vexc0
+        h = np.einsum("lr,mlj->mjr", self.v[1:], self.pl[:, 1:, :]) + s_r[None, None, :]
+        for mm in range(h.shape[0]):
+            h[mm, :mm] = 0.0
+        self.htab = h
+
     def init_potentials(self):
         """h_timePropagation.cuh:47-57: Hartree0, XC0, Hartree, XC."""
+        if self.theta:
+            if self.hartree_on:
+                self.density0 = self.theta_density(self.x)[0]
+                self.v0 = self.theta_hartree(self.density0[None, :])[0]
+            self.vexc0 = self.exchange(self.density0, clamp=False)
+            self.update_potentials()
+            return
         if self.hartree_on:
             self.density0 = self.density_multipoles(self.x)[0]
             self.v0 = self.hartree_from_density(self.density0[None, :])[0]
@@ -338,6 +462,14 @@ class OracleState:
         self.update_potentials()
 
     def update_potentials(self):
+        if self.theta:
+            if self.hartree_on:
+                dens = self.theta_density(self.x)
+                self.density = dens
+                self.v = self.theta_hartree(dens)
+                self.vexc = self.exchange(dens[0], clamp=True)
+                self.theta_table()
+            return
         if self.hartree_on:
             dens = self.density_multipoles(self.x)
             self.density[:dens.shape[0]] = dens
@@ -383,8 +515,38 @@ class OracleState:
         return dip, acc, norm
 
     # ----- one step -----
+    def _theta_half(self, x, E):
+        """x <- V_P,m diag(exp(-i dt/2 (r E x_j + H_m(r, j)))) V_P,m^T x for every orbital (the P
+        coupling of couplingP.cuh:1-125 with the whole angular potential in its phase)."""
+        p = self.p
+        V, D = p.V["P"], p.D["P"]
+        out = np.zeros_like(x)
+        for m in sorted(set(int(v) for v in p.m)):
+            ks = [k for k in range(p.n_kso) if int(p.m[k]) == m]
+            Vm = V[m][m:, m:]
+            xm = x[m:][:, ks, :].reshape(p.n_l - m, len(ks) * p.n_r)
+            xr = (Vm.T @ xm).reshape(p.n_l - m, len(ks), p.n_r)
+            eta = ((p.r[None, :] * E) * D[m, m:][:, None] + (self.htab[m, m:] if self.hartree_on else 0.0))
+            eta = (eta * (0.5 * p.dt))[:, None, :]
+            xr = (np.cos(eta) * xr.real + np.sin(eta) * xr.imag) + 1j * (np.cos(eta) * xr.imag - np.sin(eta) * xr.real)
+            out[m:, ks, :] = (Vm @ xr.reshape(p.n_l - m, len(ks) * p.n_r)).reshape(p.n_l - m, len(ks), p.n_r)
+        return out
+
+    def step_theta(self, tdx: int):
+        """One step of the theta form: angular half, radial product, angular half (the reference's
+        order, h_timePropagation.cuh:59-107, with the FF/FP/D/P/S couplings replaced by one diagonal
+        phase at the nodes), then the potentials of the new orbitals (lagging one step, as there)."""
+        E = self.p.E[tdx]
+        x = self._theta_half(self.x, E)
+        x = np.matmul(x, self.p.W)
+        self.x = self._theta_half(x, E)
+        self.update_potentials()
+        return self.observables()
+
     def step(self, tdx: int):
         """One pass of the tdx loop body (h_timePropagation.cuh:59-107)."""
+        if self.theta:
+            return self.step_theta(tdx)
         p = self.p
         h = self.hartree_on
         E = p.E[tdx]

@@ -33,3 +33,17 @@ def test_traffic_estimate_uses_the_ratio_of_each_groups_kernel():
     assert est == pytest.approx(one * r1 + two * r2)
     # no capture for this form: no estimate
     assert bench.measured_traffic(runs, groups, "fp64", "angular_second") is None
+
+
+@pytest.mark.parametrize("name,total", [("ar-ens64", 64), ("hhe-ens256", 256), ("ar16-n600", 16), ("he-fp64", 1)])
+def test_cpu_sample_covers_every_grid_group_once(name, total):
+    """The CPU legs time one run per grid group and weight it by the runs in that group."""
+    from ggbtddft_b200 import problems as P
+    groups = bench.workload_groups(name)
+    assert sum(count for _, count, _ in groups) == total
+    if name == "ar-ens64":
+        dr = P.argon_draws(64, seed=0)
+        assert len(groups) == 5                      # the five ladder rungs
+        for idx, count, _ in groups:
+            same = [i for i in range(64) if dr.rung[i] == dr.rung[idx]]
+            assert len(same) == count and idx == same[0]

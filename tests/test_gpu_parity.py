@@ -78,7 +78,7 @@ def test_fp64_pw92_correlation():
 def test_graph_replay_equals_single_steps():
     run = P.reference_like(64, 16, 80, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=1)
     a = TimePropagation([run])
-    a.step(70)                     # two graph replays of 32 steps + 6 direct steps
+    a.step(70)                     # two replays of the 32-step graph + 6 of the 1-step graph
     b = TimePropagation([run])
     for _ in range(70):
         b.step(1)
@@ -120,7 +120,7 @@ def test_step_beyond_field_sets_status_not_fault():
 @pytest.mark.parametrize("precision", ["fp64", "split_int8"])
 def test_several_grid_groups_equal_single_runs(precision):
     """Runs on three different grids (three groups, stepped on concurrent streams) give exactly the
-    results of each run stepped alone: 70 steps = two graph replays + 6 direct steps."""
+    results of each run stepped alone: 70 steps = two replays of the 32-step graph + 6 of the 1-step graph."""
     runs = [P.reference_like(48, 12, 72, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=3),
             P.reference_like(64, 16, 72, "H", r_mask=20.0),
             P.reference_like(40, 9, 72, "Ne3", r_mask=12.0, dt_as=10.0, perturb=0.02, seed=4)]
