@@ -43,6 +43,7 @@ struct GroupHost {
   unsigned* done_d = nullptr;
   bool needs_init = true;
   GroupArgs args{};
+  ThetaArgs theta_args{};        // theta form with n_har > 4 (ggb_theta.cu)
   MixedGroup mixed;              // split-precision form (ggb_mixed.cu)
   // flags shared by the runs of the group
   int n_har = 0, use_hartree = 0, target_id = 0, theta = 0;
@@ -56,6 +57,7 @@ struct RunHost {
   double *E_d = nullptr, *v_d = nullptr, *v0_d = nullptr, *vexc_d = nullptr, *vexc0_d = nullptr;
   double *rho_frozen_d = nullptr, *norm_d = nullptr, *norm0_d = nullptr;
   double2 *dip_d = nullptr, *acc_d = nullptr, *dip_tot_d = nullptr, *acc_tot_d = nullptr;
+  double* htab_d = nullptr;      // theta form with n_har > 4
   std::vector<int> l, m, occ;
 };
 
@@ -243,6 +245,106 @@ static void build_chain(GroupHost& g, const std::vector<Act>& seq, int half, int
   }
 }
 
+// Gauss-Legendre nodes and weights of order n (x_k > 0 for k < n/2, x_(n-1-k) = -x_k), Newton on
+// P_n from the Chebyshev guesses, in long double.
+static void gauss_legendre(int n, std::vector<long double>& x, std::vector<long double>& w) {
+  x.assign(n, 0.0L);
+  w.assign(n, 0.0L);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    long double z = std::cos(pi * (i + 0.75L) / (n + 0.5L)), dp = 0.0L;
+    for (int it = 0; it < 100; ++it) {
+      long double p0 = 1.0L, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const long double p2 = ((2.0L * k - 1.0L) * z * p1 - (k - 1.0L) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0L);
+      const long double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-19L) break;
+    }
+    x[i] = z;
+    x[n - 1 - i] = -z;
+    w[i] = w[n - 1 - i] = 2.0L / ((1.0L - z * z) * dp * dp);
+  }
+}
+
+// Tables and buffers of the exact multipoles of the theta form with n_har > 4 (ggb_theta.cu).
+static int prepare_theta_tables(ggb_ctx* ctx, GroupHost& g, int n_mp) {
+  const int n_l = g.d.n_l, n_m = g.d.n_m, n_r = g.d.n_r, nq = n_l, ldS = g.ldS;
+  std::vector<long double> xq, wq;
+  gauss_legendre(2 * n_l, xq, wq);   // xq[0 .. n_l-1] > 0
+  std::vector<double> T((size_t)n_m * nq * n_l, 0.0), wP((size_t)n_mp * nq), PLj((size_t)n_m * n_mp * ldS, 0.0);
+  for (int m = 0; m < n_m; ++m)
+    for (int q = 0; q < nq; ++q) {
+      // normalised associated Legendre functions of order m by the dipole coupling's recurrence
+      // x Theta_l = c_u(l) Theta_(l+1) + c_d(l) Theta_(l-1); Theta_m = C (1 - x^2)^(m/2),
+      // C^2 = (2m+1)! / (2^(2m+1) (m!)^2)
+      const long double z = xq[q];
+      long double c2 = 0.5L;
+      for (int k = 1; k <= m; ++k) c2 *= (2.0L * k + 1.0L) * (2.0L * k) / (4.0L * k * k);
+      long double tm1 = 0.0L, t0 = std::sqrt(c2) * std::pow(1.0L - z * z, 0.5L * m);
+      double* row = T.data() + ((size_t)m * nq + q) * n_l;
+      for (int l = m; l < n_l; ++l) {
+        row[l] = (double)t0;
+        if (l + 1 < n_l) {
+          const long double t1 = (z * t0 - (l > m ? (long double)h_cd(l, m) * tm1 : 0.0L)) / (long double)h_cu(l, m);
+          tm1 = t0;
+          t0 = t1;
+        }
+      }
+    }
+  for (int q = 0; q < nq; ++q) {
+    long double p0 = 1.0L, p1 = xq[q];
+    for (int L = 0; L < n_mp; ++L) {
+      const long double pl = L == 0 ? 1.0L : p1;
+      wP[(size_t)L * nq + q] = (double)(wq[q] * pl);
+      if (L >= 1) {
+        const long double p2 = ((2.0L * L + 1.0L) * xq[q] * p1 - L * p0) / (L + 1.0L);
+        p0 = p1;
+        p1 = p2;
+      }
+    }
+  }
+  for (int m = 0; m < n_m; ++m)
+    for (int j = m; j < n_l; ++j) {
+      const long double z = g.D[GGB_COUPLING_P][m][j];
+      long double p0 = 1.0L, p1 = z;
+      for (int L = 0; L < n_mp; ++L) {
+        PLj[((size_t)m * n_mp + L) * ldS + j] = (double)(L == 0 ? 1.0L : p1);
+        if (L >= 1) {
+          const long double p2 = ((2.0L * L + 1.0L) * z * p1 - L * p0) / (L + 1.0L);
+          p0 = p1;
+          p1 = p2;
+        }
+      }
+    }
+  std::vector<double> lq(n_r, 0.0);
+  for (int a = 1; a < n_r; ++a) lq[a] = (double)std::log((long double)g.r[a - 1] / (long double)g.r[a]);
+  ThetaArgs& t = g.theta_args;
+  t.n_mp = n_mp;
+  t.nq = nq;
+  double *Td, *wPd, *PLd, *lqd, *fine, *rho, *vmp;
+  int rc;
+  const size_t nrun = g.runs.size();
+  if ((rc = dalloc(ctx, &Td, T.size())) || (rc = dalloc(ctx, &wPd, wP.size())) || (rc = dalloc(ctx, &PLd, PLj.size())) ||
+      (rc = dalloc(ctx, &lqd, lq.size())) || (rc = dalloc(ctx, &fine, nrun * 2 * nq * n_r)) ||
+      (rc = dalloc(ctx, &rho, nrun * n_mp * n_r)) || (rc = dalloc(ctx, &vmp, nrun * n_mp * n_r)))
+    return rc;
+  CK(cudaMemcpy(Td, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(wPd, wP.data(), wP.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(PLd, PLj.data(), PLj.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(lqd, lq.data(), lq.size() * sizeof(double), cudaMemcpyHostToDevice));
+  t.T = Td; t.wP = wPd; t.PLj = PLd; t.lq = lqd; t.fine = fine; t.rho = rho; t.vmp = vmp;
+  for (int ri : g.runs) {
+    RunHost& r = ctx->runs[ri];
+    if ((rc = dalloc(ctx, &r.htab_d, (size_t)n_m * n_l * n_r))) return rc;
+  }
+  return GGB_OK;
+}
+
 static int prepare(ggb_ctx* ctx) {
   if (ctx->prepared) return GGB_OK;
   int n_l_max = 0, n_r_max = 0;
@@ -251,6 +353,7 @@ static int prepare(ggb_ctx* ctx) {
     n_r_max = std::max(n_r_max, g.d.n_r);
   }
   CK(configure_kernels_fp64(n_l_max, n_r_max));
+  CK(configure_theta(n_l_max));
   for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
     GroupHost& g = ctx->groups[gi];
     if (!g.grid_set) return fail(ctx, GGB_ERR_STATE, "group %zu: grid not set", gi);
@@ -299,7 +402,12 @@ static int prepare(ggb_ctx* ctx) {
     a.hartree_on = (g.use_hartree == 1 && g.target_id > 0);
     a.p_hartree = (g.use_hartree == 1 && g.n_har > 1 && g.target_id > 0);
     a.theta = g.theta;
-    a.n_den = a.hartree_on ? std::min(g.n_har, N_DEN) : 0;
+    // the theta form with n_har > 4 takes its multipoles L >= 1 from the exact quadratures of
+    // ggb_theta.cu; the angular kernels' l-space partials then only carry L = 0 (monopole, norm)
+    a.theta_tab = (g.theta && a.hartree_on && g.n_har > N_DEN) ? 1 : 0;
+    a.n_den = a.hartree_on ? (a.theta_tab ? 1 : std::min(g.n_har, N_DEN)) : 0;
+    if (a.theta_tab)
+      if ((rc = prepare_theta_tables(ctx, g, g.n_har))) return rc;
     a.per_l = ctx->dims.per_l;
     a.dt = g.dt;
     // the FP64 form never raises a norm (its propagators are contractions, rounding is ~1e-15); the
@@ -326,7 +434,8 @@ static int prepare(ggb_ctx* ctx) {
     if (!r.orb_set) return fail(ctx, GGB_ERR_STATE, "run %zu: orbitals not set", i);
     if (!r.field_set) return fail(ctx, GGB_ERR_STATE, "run %zu: field not set", i);
     rd[i] = RunDev{r.E_d, r.v_d, r.v0_d, r.vexc_d, r.vexc0_d, r.rho_frozen_d, r.dip_d, r.acc_d,
-                   r.dip_tot_d, r.acc_tot_d, r.norm_d, r.norm0_d, r.col0, r.d.n_orb, ctx->dims.n_t, r.d.flags};
+                   r.dip_tot_d, r.acc_tot_d, r.norm_d, r.norm0_d, r.htab_d, r.col0, r.d.n_orb, ctx->dims.n_t,
+                   r.d.flags};
   }
   CK(cudaMemcpy(ctx->runs_dev, rd.data(), rd.size() * sizeof(RunDev), cudaMemcpyHostToDevice));
   ctx->prepared = true;
@@ -343,6 +452,7 @@ static void launch_group_step(ggb_ctx* ctx, GroupHost& g, cudaStream_t s) {
   } else {
     mixed_step(g.mixed, a, s);
   }
+  if (a.theta_tab) launch_theta_potentials(a, g.theta_args, g.x_d, s);
   launch_finalize(a, 1, s);
 }
 
@@ -382,6 +492,7 @@ static int launch_init(ggb_ctx* ctx, GroupHost& g, cudaStream_t s) {
     mixed_init(g.mixed, a, g.x_d, s);
   }
   launch_finalize(a, 0, s);
+  if (a.theta_tab) launch_theta_potentials(a, g.theta_args, g.x_d, s);
   CK(cudaGetLastError());
   g.needs_init = false;
   return GGB_OK;
@@ -431,7 +542,7 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     GroupHost& g = ctx->groups[r.d.group];
     const int theta = (r.d.flags & GGB_RUN_THETA) ? 1 : 0;
     if (theta && dims->precision == GGB_SPLIT_BF16) return bad(GGB_ERR_ARG, "theta form with split_bf16");
-    if (theta && r.d.n_har > N_DEN) return bad(GGB_ERR_ARG, "theta form: n_har > 4");
+    if (theta && r.d.n_har > 2 * groups[r.d.group].n_l - 1) return bad(GGB_ERR_ARG, "theta form: n_har > 2 l_max + 1");
     if (!g.runs.empty()) {
       if (g.n_har != r.d.n_har || g.use_hartree != r.d.use_hartree || (g.target_id > 0) != (r.d.target_id > 0) ||
           g.dt != r.d.dt || g.theta != theta)
@@ -643,7 +754,10 @@ int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream) {
     } else {
       mixed_phase(g.mixed, a, phase, s);
     }
-    if (phase == 3) launch_finalize(a, 2, s);
+    if (phase == 3) {
+      if (a.theta_tab) launch_theta_potentials(a, g.theta_args, g.x_d, s);
+      launch_finalize(a, 2, s);
+    }
   }
   CK(cudaGetLastError());
   return GGB_OK;
@@ -702,6 +816,15 @@ int ggb_get_potentials(ggb_ctx* ctx, int run, double* v, double* v0, double* vex
   const int nr = ctx->groups[r.d.group].d.n_r;
   CK(cudaDeviceSynchronize());
   if (v) CK(cudaMemcpy(v, r.v_d, 4 * (size_t)nr * sizeof(double), cudaMemcpyDefault));
+  const GroupHost& g = ctx->groups[r.d.group];
+  if (v && g.args.theta_tab) {
+    // the theta form with n_har > 4 keeps its multipoles L >= 1 in the exact-quadrature buffers
+    const int ri = (int)(std::find(g.runs.begin(), g.runs.end(), run) - g.runs.begin());
+    const int rows = std::min(g.theta_args.n_mp, 4) - 1;
+    if (rows > 0)
+      CK(cudaMemcpy(v + nr, g.theta_args.vmp + ((size_t)ri * g.theta_args.n_mp + 1) * nr, (size_t)rows * nr * sizeof(double),
+                    cudaMemcpyDefault));
+  }
   if (v0) CK(cudaMemcpy(v0, r.v0_d, nr * sizeof(double), cudaMemcpyDefault));
   if (vexc) CK(cudaMemcpy(vexc, r.vexc_d, nr * sizeof(double), cudaMemcpyDefault));
   if (vexc0) CK(cudaMemcpy(vexc0, r.vexc0_d, nr * sizeof(double), cudaMemcpyDefault));

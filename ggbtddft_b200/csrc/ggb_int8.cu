@@ -741,7 +741,12 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int p = p0 + u;
-          if (th) v[u] = rotd(v[u], pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p]);
+          if (th) {
+            double ang = pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p];
+            // n_har > 4: the multipoles L >= 1 at this node come from the exact-quadrature table
+            if (g.theta_tab && r0 + p < g.n_r) ang += run.htab[((size_t)m * n_l + j) * g.n_r + r0 + p] * hdt;
+            v[u] = rotd(v[u], ang);
+          }
           else if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
           if (post_s) v[u] = rotd(v[u], pbase[4][p] + pj * pbase[2][p]);
           if (!last) {

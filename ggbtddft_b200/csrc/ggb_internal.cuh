@@ -67,6 +67,7 @@ struct RunDev {
   double2* acc_tot;
   double* norm;           // [n_orb][n_t]
   double* norm0;          // [n_orb] norm at t = 0 (for the growth watchdog)
+  double* htab;           // theta form with n_har > 4: sum_{L>=1} v_L(r) P_L(x_j^m), [N_m][N_l][N_r]
   int col0;
   int n_orb;
   int n_t;
@@ -76,6 +77,7 @@ struct RunDev {
 struct GroupArgs {
   int n_r, n_l, n_m, n_cols, n_tiles, ldS, n_runs;
   int theta;        // theta form (GGB_RUN_THETA): one phase per half-step at the P nodes
+  int theta_tab;    // theta form with n_har > 4: the multipoles L >= 1 come from run.htab
   int hartree_on;   // USE_HARTREE == 1 && targetID > 0
   int p_hartree;    // P phase carries v_1 (USE_HARTREE && N_har > 1 && targetID > 0)
   int n_den;        // multipoles computed: min(N_har, 4) when hartree_on, else 0
@@ -102,6 +104,23 @@ struct GroupArgs {
   unsigned* done;           // block counter for the last-block step increment
   Chain chain[3];   // first half, second half, empty (initial partials)
 };
+
+// Exact multipoles L = 0 .. n_mp-1 of the theta form with n_har > 4 (ggb_theta.cu).  Fine
+// Gauss-Legendre quadrature on 2 N_l nodes +-x_q (q < nq = N_l, x_q > 0), using the parity of the
+// normalised associated Legendre functions Theta_l^m(-x) = (-1)^(l-m) Theta_l^m(x).
+struct ThetaArgs {
+  int n_mp;            // multipoles L = 0 .. n_mp-1 (<= 2 N_l - 1)
+  int nq;              // positive fine nodes (= N_l)
+  const double* T;     // [N_m][nq][N_l]  Theta_l^m(x_q)
+  const double* wP;    // [n_mp][nq]      w_q P_L(x_q)
+  const double* PLj;   // [N_m][n_mp][ldS] P_L(x_j^m) at the P coupling's nodes
+  const double* lq;    // [N_r]           log(r_(a-1) / r_a) for a >= 1, 0 at a = 0
+  double* fine;        // [n_runs][2][nq][N_r]  S_q = sum occ 2(|E|^2 + |O|^2), D_q = sum occ 4 Re(E conj O)
+  double* rho;         // [n_runs][n_mp][N_r]
+  double* vmp;         // [n_runs][n_mp][N_r]
+};
+void launch_theta_potentials(const GroupArgs& g, const ThetaArgs& t, const double2* x, cudaStream_t s);
+cudaError_t configure_theta(int n_l_max);
 
 __device__ __forceinline__ double2 cmul_conj_phase(double2 x, double eta) {
   // x * exp(-i eta) written as the reference's phase kernels do (couplingP.cuh:99-102)

@@ -128,6 +128,8 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
             // the theta form: the whole angular potential at node x_j
             const double xj = Dv[j];
             double eta = (rr * E + v1) * xj + v2 * legendre_p2(xj) + v3 * legendre_p3(xj) + sbase;
+            // n_har > 4: the multipoles L >= 1 at this node come from the exact-quadrature table
+            if (g.theta_tab && rv) eta += run.htab[((size_t)m * n_l + j) * g.n_r + r];
             eta *= hdt;
             y = cmul_conj_phase(y, eta);
           } else if (op.phase != PH_NONE && j >= m) {
