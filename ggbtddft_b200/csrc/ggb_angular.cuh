@@ -139,7 +139,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Dipole and acceleration partial sums for every l of one column over the radii r0 + lane held by
-// a warp (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc): one
+// a lane group -- a warp, or half of one with seg = 16, the halves on different l
+// (dipoleMoment.cuh:19-43 / dipoleAcceleration.cuh:17-41 followed by cublasZdotc): one
 // partial per g.obs_seg consecutive radii (32 or 16), index (r0 + lane) / g.obs_seg.  Lanes from
 // n_valid on hold no radius.
 // COMPENSATED: double-double sums (the FP64 form, held to 1e-10 of the reference); otherwise plain
@@ -155,9 +156,14 @@ __device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m
   const bool lv = lane < n_valid;
   const double* cu = cu_row ? cu_row : g.coef + ((size_t)CF_CU * g.n_m + m) * n_l;
   const double* cd = cd_row ? cd_row : g.coef + ((size_t)CF_CD * g.n_m + m) * n_l;
-  for (int l = warp; l < n_l; l += n_warps) {
+  // every lane runs the same number of iterations (the shuffles below span the whole warp, whose
+  // lane groups may hold different l)
+  const int iters = (n_l + n_warps - 1) / n_warps;
+  for (int it = 0; it < iters; ++it) {
+    const int l = warp + it * n_warps;
+    const bool lok = l < n_l;
     double4 out = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (l >= m && lv) {
+    if (lok && l >= m && lv) {
       const double2 xl = to_d2(xs[l * STRIDE + lane]);
       const double2 xu = (l + 1 < n_l) ? to_d2(xs[(l + 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
       const double2 xd = (l >= 1) ? to_d2(xs[(l - 1) * STRIDE + lane]) : make_double2(0.0, 0.0);
@@ -194,7 +200,7 @@ __device__ void observables_tile(const GroupArgs& g, const C* xs, int col, int m
       }
       sx = dd{out.x, 0.0}; sy = dd{out.y, 0.0}; sz = dd{out.z, 0.0}; sw = dd{out.w, 0.0};
     }
-    if (lv && (lane & (seg - 1)) == 0) {
+    if (lok && lv && (lane & (seg - 1)) == 0) {
       double4* o = g.obs + 2 * (((size_t)col * n_l + l) * g.n_tiles + (r0 + lane) / seg);
       o[0] = make_double4(sx.hi, sy.hi, sz.hi, sw.hi);
       o[1] = make_double4(sx.lo, sy.lo, sz.lo, sw.lo);

@@ -10,14 +10,22 @@
 //                  orbitals (hartreePotentialDensity.cuh:1-181, dipoleMoment.cuh:1-75,
 //                  dipoleAcceleration.cuh:1-71), so the orbitals are read once per half-step.
 //  k_radial_fp64   x_l <- A_l x_l for every l with A_l(a,b) = W[l][b][a]: the batched ZGEMM of
-//                  h_propagationH0 (h_timePropagation.cuh:1-30), out of place.
+//                  h_propagationH0 (h_timePropagation.cuh:1-30), out of place.  Persistent, two CTAs
+//                  per SM; a producer warp streams the W rows and x segments of each 32-wide k chunk
+//                  into a 3-stage shared-memory ring with cp.async.bulk (mbarrier transaction
+//                  counts), so that ~200 KB per SM are in flight whatever the occupancy; four
+//                  consumer warps (one output radius per thread, TC orbital columns in registers)
+//                  run the FP64 FMAs from shared memory.
 //  k_finalize      per run: observables of the step from the partials, density multipoles
 //                  (occupation-weighted sum over orbitals), Hartree potentials by compensated
 //                  prefix scans (h_calculateHartreePotential.cuh:1-136), LDA exchange
 //                  (h_calculateExchangeCorrelationPotential.cuh:1-56), step counter.
+#include <algorithm>
 #include <cstdio>
 #include "ggb_internal.cuh"
 #include "ggb_angular.cuh"
+#include "ggb_mixed.cuh"
+#include "ggb_tc_common.cuh"
 
 namespace ggb {
 
@@ -27,26 +35,33 @@ namespace ggb {
 
 constexpr int ANG_JB = 8;   // eigen-channels j per register block
 
+// RT radii per CTA (32, or 16 with the two half-warps on different eigen-channel blocks): lane % RT is
+// the radius, lane / RT picks the half; the group's observables partials cover RT radii each.
+template <int RT>
 __global__ void __launch_bounds__(ANG_WARPS * 32)
 k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* __restrict__ xout, int do_obs) {
-  extern __shared__ double2 sm[];  // two [N_l][TR] buffers
+  constexpr int SUB = 32 / RT;                    // lanes groups per warp (1 or 2)
+  constexpr int NSUB = ANG_WARPS * SUB;           // thread groups that stride l and j
+  extern __shared__ double2 sm[];  // two [N_l][RT] buffers
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int tiles32 = (g.n_r + TR - 1) / TR;     // this kernel's CTAs cover 32 radii each
-  const int col = blockIdx.x / tiles32;
-  const int tile = blockIdx.x - col * tiles32;
-  const int r = tile * TR + lane;
+  const int lr = lane % RT;                       // radius of this lane
+  const int sub = warp * SUB + lane / RT;         // this thread's group
+  const int tilesN = (g.n_r + RT - 1) / RT;
+  const int col = blockIdx.x / tilesN;
+  const int tile = blockIdx.x - col * tilesN;
+  const int r = tile * RT + lr;
   const bool rv = r < g.n_r;
   const int n_l = g.n_l;
   double2* xs = sm;
-  double2* ys = sm + (size_t)n_l * TR;
+  double2* ys = sm + (size_t)n_l * RT;
   const int m = g.col_m[col];
   const RunDev run = g.runs[g.col_run[col]];
   int step = *g.step;
   if (step >= run.n_t) step = run.n_t - 1;  // overflow is flagged by k_finalize
 
-  for (int l = warp; l < n_l; l += ANG_WARPS)
-    xs[l * TR + lane] = rv ? xin[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
+  for (int l = sub; l < n_l; l += NSUB)
+    xs[l * RT + lr] = rv ? xin[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
 
   // per-radius potentials
   const double rr = rv ? g.r[r] : 1.0;
@@ -66,10 +81,10 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
 
   const Chain& ch = g.chain[half];
   if (ch.pre_s) {
-    for (int l = warp; l < n_l; l += ANG_WARPS) {
+    for (int l = sub; l < n_l; l += NSUB) {
       double eta = sbase + pco[l] * v2;
       eta *= hdt;
-      xs[l * TR + lane] = cmul_conj_phase(xs[l * TR + lane], eta);
+      xs[l * RT + lr] = cmul_conj_phase(xs[l * RT + lr], eta);
     }
     __syncthreads();
   }
@@ -83,7 +98,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
     else if (op.phase == PH_D) base = v2;
     else if (op.phase != PH_NONE) base = v3;  // FP and FF
     const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
-    for (int j0 = warp * ANG_JB; j0 < n_l; j0 += ANG_WARPS * ANG_JB) {
+    for (int j0 = sub * ANG_JB; j0 < n_l; j0 += NSUB * ANG_JB) {
       double2 acc[ANG_JB];
 #pragma unroll
       for (int q = 0; q < ANG_JB; ++q) acc[q] = make_double2(0.0, 0.0);
@@ -95,7 +110,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
         double2 xv[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          xv[u] = xs[(l + u) * TR + lane];
+          xv[u] = xs[(l + u) * RT + lr];
           const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)(l + u) * g.ldS);
 #pragma unroll
           for (int h = 0; h < ANG_JB / 2; ++h) sv[u][h] = __ldg(Srow + h);
@@ -109,7 +124,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
           }
       }
       for (; l < n_l; ++l) {
-        const double2 xv = xs[l * TR + lane];
+        const double2 xv = xs[l * RT + lr];
         const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)l * g.ldS);
 #pragma unroll
         for (int h = 0; h < ANG_JB / 2; ++h) {
@@ -142,7 +157,7 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
             eta *= hdt;
             y = cmul_conj_phase(y, eta);
           }
-          ys[j * TR + lane] = y;
+          ys[j * RT + lr] = y;
         }
       }
     }
@@ -151,14 +166,14 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
   }
 
   if (rv && xout)
-    for (int l = warp; l < n_l; l += ANG_WARPS) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * TR + lane];
+    for (int l = sub; l < n_l; l += NSUB) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * RT + lr];
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile(g, xs, col, m, tile * TR, lane, warp, ANG_WARPS, rr, fr2);
+    observables_tile<double2, RT>(g, xs, col, m, tile * RT, lr, sub, NSUB, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
-    for (int L = warp; L < n_den; L += ANG_WARPS) {
-      const double d = density_multipole(L, m, n_l, xs, lane, g.coef, g.n_m);
+    for (int L = sub; L < n_den; L += NSUB) {
+      const double d = density_multipole<double2, RT>(L, m, n_l, xs, lr, g.coef, g.n_m);
       if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
     }
   }
@@ -168,70 +183,154 @@ size_t angular_smem_fp64(int n_l) { return 2 * (size_t)n_l * TR * sizeof(double2
 
 void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
                          cudaStream_t s) {
-  const dim3 grid(g.n_cols * ((g.n_r + TR - 1) / TR)), block(ANG_WARPS * 32);
-  const size_t smem = angular_smem_fp64(g.n_l);
-  k_angular_fp64<<<grid, block, smem, s>>>(g, half, xin, xout, do_obs);
+  const dim3 block(ANG_WARPS * 32);
+  if (g.obs_seg == 16) {
+    const dim3 grid(g.n_cols * ((g.n_r + 15) / 16));
+    k_angular_fp64<16><<<grid, block, 2 * (size_t)g.n_l * 16 * sizeof(double2), s>>>(g, half, xin, xout, do_obs);
+  } else {
+    const dim3 grid(g.n_cols * ((g.n_r + TR - 1) / TR));
+    k_angular_fp64<TR><<<grid, block, angular_smem_fp64(g.n_l), s>>>(g, half, xin, xout, do_obs);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
 // radial propagator, FP64
 // ---------------------------------------------------------------------------------------------
 
-constexpr int RAD_TI = 128;   // rows per CTA
-constexpr int RAD_KC = 32;    // k chunk staged in shared memory
+constexpr int RAD_CW = 2;                 // consumer warps: one output radius per thread
+constexpr int RAD_TI = 32 * RAD_CW;       // rows (output radii) per tile
+constexpr int RAD_KC = 32;                // k per stage
+constexpr int RAD_STAGES = 3;
+constexpr int RAD_THREADS = 32 * (RAD_CW + 1);
 
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Tiles (l, radius tile, column tile), the column tile fastest so that CTAs running side by side
+// read the same W rows (one HBM read, the others from L2).
 template <int TC>
-__global__ void __launch_bounds__(RAD_TI)
-k_radial_fp64(int n_r, int n_cols, const double2* __restrict__ W, const double2* __restrict__ xin,
-              double2* __restrict__ xout) {
-  __shared__ double2 xsm[TC][RAD_KC];
-  const int l = blockIdx.z;
-  const int i = blockIdx.x * RAD_TI + threadIdx.x;
-  const int c0 = blockIdx.y * TC;
-  const bool iv = i < n_r;
-  const double2* Wl = W + (size_t)l * n_r * n_r;
-  const double2* Xl = xin + (size_t)l * n_cols * n_r;
-  double2 acc[TC];
-#pragma unroll
-  for (int c = 0; c < TC; ++c) acc[c] = make_double2(0.0, 0.0);
-  for (int k0 = 0; k0 < n_r; k0 += RAD_KC) {
-    for (int idx = threadIdx.x; idx < TC * RAD_KC; idx += RAD_TI) {
-      const int c = idx / RAD_KC, kk = idx - c * RAD_KC;
-      xsm[c][kk] = (c0 + c < n_cols && k0 + kk < n_r) ? Xl[(size_t)(c0 + c) * n_r + k0 + kk] : make_double2(0.0, 0.0);
+__global__ void __launch_bounds__(RAD_THREADS, 2)
+k_radial_fp64(int n_r, int n_cols, int n_l, const double2* __restrict__ W, const double2* __restrict__ xin,
+              double2* __restrict__ xout, unsigned* status) {
+  constexpr int W_STAGE = RAD_KC * RAD_TI;        // double2 per stage: [k][row]
+  constexpr int X_STAGE = TC * RAD_KC;            // [col][k]
+  extern __shared__ __align__(128) double2 rsm[];
+  __shared__ uint64_t full_bar[RAD_STAGES], empty_bar[RAD_STAGES];
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_it = (n_r + RAD_TI - 1) / RAD_TI, n_ct = (n_cols + TC - 1) / TC;
+  const int total = n_it * n_ct * n_l;
+  const int n_kc = (n_r + RAD_KC - 1) / RAD_KC;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < RAD_STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], RAD_CW);
     }
-    __syncthreads();
-    const int kmax = min(RAD_KC, n_r - k0);
-    int kk = 0;
-    // eight W loads in flight per thread before the FMAs that consume them
-    for (; kk + 8 <= kmax; kk += 8) {
-      double2 w[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) w[u] = iv ? __ldcs(Wl + (size_t)(k0 + kk + u) * n_r + i) : make_double2(0.0, 0.0);
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int c = 0; c < TC; ++c) {
-          const double2 x = xsm[c][kk + u];
-          acc[c].x += w[u].x * x.x - w[u].y * x.y;
-          acc[c].y += w[u].x * x.y + w[u].y * x.x;
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  volatile int* abort_p = &abort_flag;
+  if (warp == RAD_CW) {
+    // producer: one thread issues the bulk copies of every stage
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+        const int ct = tile % n_ct, rest = tile / n_ct, itile = rest % n_it, l = rest / n_it;
+        const int i0 = itile * RAD_TI, rows = min(RAD_TI, n_r - i0);
+        const int c0 = ct * TC, nc = min(TC, n_cols - c0);
+        const double2* Wl = W + (size_t)l * n_r * n_r;
+        const double2* Xl = xin + (size_t)l * n_cols * n_r;
+        for (int kc = 0; kc < n_kc; ++kc, ++it) {
+          const int s = it % RAD_STAGES;
+          if (it >= RAD_STAGES && !mbar_wait(&empty_bar[s], ((it / RAD_STAGES) & 1) ^ 1, abort_p)) {
+            ok = false;
+            break;
+          }
+          const int k0 = kc * RAD_KC, kn = min(RAD_KC, n_r - k0);
+          double2* ws = rsm + (size_t)s * (W_STAGE + X_STAGE);
+          double2* xs = ws + W_STAGE;
+          mbar_expect_tx(&full_bar[s], (uint32_t)(kn * rows + nc * kn) * 16u);
+          for (int kk = 0; kk < kn; ++kk)
+            bulk_g2s(ws + kk * RAD_TI, Wl + (size_t)(k0 + kk) * n_r + i0, (uint32_t)rows * 16u, &full_bar[s]);
+          for (int c = 0; c < nc; ++c)
+            bulk_g2s(xs + c * RAD_KC, Xl + (size_t)(c0 + c) * n_r + k0, (uint32_t)kn * 16u, &full_bar[s]);
         }
-    }
-    for (; kk < kmax; ++kk) {
-      const double2 w = iv ? __ldcs(Wl + (size_t)(k0 + kk) * n_r + i) : make_double2(0.0, 0.0);
-#pragma unroll
-      for (int c = 0; c < TC; ++c) {
-        const double2 x = xsm[c][kk];
-        acc[c].x += w.x * x.x - w.y * x.y;
-        acc[c].y += w.x * x.y + w.y * x.x;
+      }
+      if (!ok) {
+        // let the copies already issued land before the CTA exits
+        for (int q = (it > RAD_STAGES ? it - RAD_STAGES : 0); q < it; ++q)
+          mbar_drain(&full_bar[q % RAD_STAGES], (q / RAD_STAGES) & 1);
       }
     }
-    __syncthreads();
-  }
-  if (iv)
+  } else {
+    // consumers: thread t computes output radius i0 + t for the tile's TC columns
+    const int t = threadIdx.x;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+      const int ct = tile % n_ct, rest = tile / n_ct, itile = rest % n_it, l = rest / n_it;
+      const int i0 = itile * RAD_TI;
+      const int c0 = ct * TC, nc = min(TC, n_cols - c0);
+      double2 acc[TC];
 #pragma unroll
-    for (int c = 0; c < TC; ++c)
-      if (c0 + c < n_cols) xout[((size_t)l * n_cols + c0 + c) * n_r + i] = acc[c];
+      for (int c = 0; c < TC; ++c) acc[c] = make_double2(0.0, 0.0);
+      bool ok = true;
+      for (int kc = 0; kc < n_kc; ++kc, ++it) {
+        const int s = it % RAD_STAGES;
+        if (!mbar_wait(&full_bar[s], (it / RAD_STAGES) & 1, abort_p)) {
+          ok = false;
+          break;
+        }
+        const int kn = min(RAD_KC, n_r - kc * RAD_KC);
+        const double2* ws = rsm + (size_t)s * (W_STAGE + X_STAGE);
+        const double2* xs = ws + W_STAGE;
+        if (kn == RAD_KC) {
+#pragma unroll 4
+          for (int kk = 0; kk < RAD_KC; ++kk) {
+            const double2 w = ws[kk * RAD_TI + t];
+#pragma unroll
+            for (int c = 0; c < TC; ++c) {
+              const double2 x = xs[c * RAD_KC + kk];
+              acc[c].x = fma(w.x, x.x, fma(-w.y, x.y, acc[c].x));
+              acc[c].y = fma(w.x, x.y, fma(w.y, x.x, acc[c].y));
+            }
+          }
+        } else {
+          for (int kk = 0; kk < kn; ++kk) {
+            const double2 w = ws[kk * RAD_TI + t];
+#pragma unroll
+            for (int c = 0; c < TC; ++c) {
+              const double2 x = xs[c * RAD_KC + kk];
+              acc[c].x = fma(w.x, x.x, fma(-w.y, x.y, acc[c].x));
+              acc[c].y = fma(w.x, x.y, fma(w.y, x.x, acc[c].y));
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty_bar[s]);
+      }
+      if (!ok) break;
+      const int i = i0 + t;
+      if (i < n_r)
+#pragma unroll
+        for (int c = 0; c < TC; ++c)
+          if (c < nc) xout[((size_t)l * n_cols + c0 + c) * n_r + i] = acc[c];
+    }
+  }
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicOr(status, ST_TC_TIMEOUT);
 }
+
+template <int TC>
+static constexpr size_t radial_fp64_smem() {
+  return (size_t)RAD_STAGES * (RAD_KC * RAD_TI + TC * RAD_KC) * sizeof(double2);
+}
+
+static int g_radial_sms = 0;
 
 void launch_radial_fp64(const GroupArgs& g, const double2* W, const double2* xin, double2* xout, cudaStream_t s) {
   const int nc = g.n_cols;
@@ -239,15 +338,34 @@ void launch_radial_fp64(const GroupArgs& g, const double2* W, const double2* xin
   static const int opts[] = {1, 2, 3, 4, 6, 8, 9, 12, 16};
   for (int o : opts)
     if (o >= tc) { tc = o; break; }
-  const dim3 grid((g.n_r + RAD_TI - 1) / RAD_TI, (nc + tc - 1) / tc, g.n_l), block(RAD_TI);
-#define GGB_RAD_CASE(C) \
-  case C: k_radial_fp64<C><<<grid, block, 0, s>>>(g.n_r, nc, W, xin, xout); break;
+  const int tiles = ((g.n_r + RAD_TI - 1) / RAD_TI) * ((nc + tc - 1) / tc) * g.n_l;
+  const int ctas = std::min(tiles, 2 * g_radial_sms);
+#define GGB_RAD_CASE(C)                                                                                     \
+  case C:                                                                                                   \
+    k_radial_fp64<C><<<ctas, RAD_THREADS, radial_fp64_smem<C>(), s>>>(g.n_r, nc, g.n_l, W, xin, xout, g.status); \
+    break;
   switch (tc) {
     GGB_RAD_CASE(1) GGB_RAD_CASE(2) GGB_RAD_CASE(3) GGB_RAD_CASE(4) GGB_RAD_CASE(6)
     GGB_RAD_CASE(8) GGB_RAD_CASE(9) GGB_RAD_CASE(12) GGB_RAD_CASE(16)
     default: break;
   }
 #undef GGB_RAD_CASE
+}
+
+static cudaError_t configure_radial_fp64() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&g_radial_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+#define GGB_RAD_ATTR(C)                                                                                   \
+  e = cudaFuncSetAttribute((const void*)k_radial_fp64<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                           (int)radial_fp64_smem<C>());                                                   \
+  if (e != cudaSuccess) return e;
+  GGB_RAD_ATTR(1) GGB_RAD_ATTR(2) GGB_RAD_ATTR(3) GGB_RAD_ATTR(4) GGB_RAD_ATTR(6)
+  GGB_RAD_ATTR(8) GGB_RAD_ATTR(9) GGB_RAD_ATTR(12) GGB_RAD_ATTR(16)
+#undef GGB_RAD_ATTR
+  return cudaSuccess;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -509,7 +627,11 @@ cudaError_t configure_kernels_fp64(int n_l_max, int n_r_max) {
   if (e != cudaSuccess) return e;
   if (angular_smem_fp64(n_l_max) > (size_t)optin || 3 * (size_t)n_r_max * sizeof(double) > (size_t)optin)
     return cudaErrorInvalidValue;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64, optin);
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR>, optin);
+  if (e != cudaSuccess) return e;
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<16>, optin);
+  if (e != cudaSuccess) return e;
+  e = configure_radial_fp64();
   if (e != cudaSuccess) return e;
   return set_max_dynamic_smem((const void*)k_finalize, optin);
 }
