@@ -10,6 +10,8 @@
 // context keeps in buffers it allocates, live here in a file-scope __device__ array of fixed size.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "../../include/ggbtddft.h"
 #include "ggb_angular.cuh"
 
@@ -52,7 +54,11 @@ k_obs_partials(const double2* __restrict__ x, const double* __restrict__ r, cons
   if (m < 0 || m > n_l) m = n_l;   // an invalid m contributes nothing (no l satisfies l >= m)
   const double rr = rv ? r[rr_i] : 1.0;
   const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-  observables_tile(g, xs, k, m, tile * TR, lane, warp, NA_WARPS, rr, fr2);
+  // the coefficient rows of this m, NA_MAX_NL long whatever the call's N_l
+  const int mr = m < NA_MAX_NL ? m : NA_MAX_NL - 1;
+  const double* cu_row = coef + ((size_t)CF_CU * NA_MAX_NL + mr) * NA_MAX_NL;
+  const double* cd_row = coef + ((size_t)CF_CD * NA_MAX_NL + mr) * NA_MAX_NL;
+  observables_tile(g, xs, k, m, tile * TR, lane, warp, NA_WARPS, rr, fr2, TR, cu_row, cd_row);
   if (warp == 0) {
     dd s{0.0, 0.0};
     for (int l = m; l < n_l; ++l) {
@@ -93,13 +99,15 @@ __global__ void k_obs_reduce(const double4* __restrict__ obs, const double2* __r
   }
 }
 
-// Angular coefficient rows c_u, c_d (m < NA_MAX_NL) of the observables, laid out [coef][m][N_l] for
-// the call's N_l: the same closed forms as the context's tables (angularCoefficients.cuh:57-111).
+// Angular coefficient rows c_u, c_d (l, m < NA_MAX_NL) of the observables, [coef][m][l] with rows
+// NA_MAX_NL long (independent of a call's N_l, so filled once per device): the same closed forms
+// as the context's tables (angularCoefficients.cuh:57-111).
 static __device__ __align__(256) double g_coef[2 * NA_MAX_NL * NA_MAX_NL];
 
-__global__ void k_fill_coef(double* coef, int n_l) {
+__global__ void k_fill_coef(double* coef) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= NA_MAX_NL * n_l) return;
+  if (i >= NA_MAX_NL * NA_MAX_NL) return;
+  const int n_l = NA_MAX_NL;
   const int m = i / n_l, l = i - m * n_l;
   const double dl = l, dm = m;
   const double cu = (l >= m) ? sqrt((pow(dl + 1.0, 2.0) - pow(dm, 2.0)) / ((2.0 * dl + 1.0) * (2.0 * dl + 3.0))) : 0.0;
@@ -117,8 +125,12 @@ struct NoallocDevice {
   double* coef = nullptr;
 };
 static NoallocDevice g_dev[64];
+static std::mutex g_setup_mutex;
 
+// Resolves the arrays' device addresses with `dev` current and fills the coefficient table, once
+// per device (synchronously); serialised across host threads.
 static int noalloc_setup(int dev) {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
   NoallocDevice& d = g_dev[dev];
   if (d.ready) return GGB_OK;
   if (cudaGetSymbolAddress((void**)&d.obs, g_obs_scratch) != cudaSuccess) return GGB_ERR_CUDA;
@@ -127,6 +139,8 @@ static int noalloc_setup(int dev) {
   if (cudaFuncSetAttribute(k_obs_partials, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            NA_MAX_NL * TR * (int)sizeof(double2)) != cudaSuccess)
     return GGB_ERR_CUDA;
+  k_fill_coef<<<(NA_MAX_NL * NA_MAX_NL + 255) / 256, 256>>>(d.coef);
+  if (cudaStreamSynchronize(0) != cudaSuccess) return GGB_ERR_CUDA;
   d.ready = true;
   return GGB_OK;
 }
@@ -147,7 +161,6 @@ extern "C" int ggb_observables_noalloc(const double* x, const double* r, const i
   if (rc) return rc;
   const NoallocDevice& d = g_dev[dev];
   cudaStream_t s = (cudaStream_t)stream;
-  k_fill_coef<<<(NA_MAX_NL * n_l + 255) / 256, 256, 0, s>>>(d.coef, n_l);
   k_obs_partials<<<n_orb * n_tiles, NA_WARPS * 32, (size_t)n_l * TR * sizeof(double2), s>>>(
       reinterpret_cast<const double2*>(x), r, d.coef, m, n_l, n_orb, n_r, n_tiles, d.obs, d.norm);
   const int nt = n_l * n_orb > n_orb ? n_l * n_orb : n_orb;

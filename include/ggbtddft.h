@@ -178,8 +178,9 @@ void ggb_destroy(ggb_ctx* ctx);
    (5.25 MiB, held on every device that loads the library until the process exits) that all calls
    share: calls that overlap on the GPU (other streams or threads) race, so serialise them.  Each
    call writes every partial it reads, so nothing has to start at zero.  The first call on a device
-   looks up the arrays' device addresses (cudaGetSymbolAddress) with that device current: make that
-   first call before any stream capture. */
+   looks up the arrays' device addresses (cudaGetSymbolAddress) with that device current and fills
+   a table of angular coefficients (synchronously): make that first call before any stream
+   capture. */
 int ggb_observables_noalloc(const double* x, const double* r, const int* m, int n_l, int n_orb, int n_r,
                             double* dip, double* acc, double* norm, void* stream);
 
