@@ -34,6 +34,7 @@ constexpr unsigned ST_NORM_GROWTH = 4u;
 enum PhaseKind { PH_NONE = 0, PH_P = 1, PH_FP = 2, PH_D = 3, PH_FF = 4, PH_THETA = 5 };
 constexpr int RUN_FLAG_PW92 = 1;
 constexpr int RUN_FLAG_THETA = 2;
+constexpr int RUN_FLAG_XC_FROZEN = 4;
 
 // P_2 and P_3 of the theta phase
 __host__ __device__ __forceinline__ double legendre_p2(double x) { return 0.5 * (3.0 * x * x - 1.0); }

@@ -583,7 +583,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
         const double lg = log1p(1.0 / q1);
         vx += q0 * lg - rs / 3.0 * (-2.0 * a * a1 * lg - q0 * q1p / (q1 * q1 + q1));
       }
-      run.vexc[q] = vx;
+      // GGB_RUN_XC_FROZEN: the exchange-correlation potential stays at its t = 0 value
+      run.vexc[q] = (run.flags & RUN_FLAG_XC_FROZEN) ? run.vexc0[q] : vx;
     }
   }
 

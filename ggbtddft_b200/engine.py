@@ -27,6 +27,7 @@ PRECISIONS = {"fp64": 0, "split_bf16": 1, "split_tf32": 2, "split_int8": 3}
 COUPLING_IDS = {"P": 0, "FP": 1, "D": 2, "FF": 3}
 RUN_XC_PW92 = 1
 RUN_THETA = 2
+RUN_XC_FROZEN = 4
 
 
 class GGBError(RuntimeError):
@@ -159,7 +160,8 @@ class TimePropagation:
         for i, r in enumerate(self.runs):
             rd[i] = _RunDesc(run_group[i], r.n_orb, r.n_har, r.use_hartree, r.target_id,
                              (RUN_XC_PW92 if r.xc_correlation else 0) |
-                             (RUN_THETA if getattr(r, "angular", "reference") == "theta" else 0), r.dt)
+                             (RUN_THETA if getattr(r, "angular", "reference") == "theta" else 0) |
+                             (RUN_XC_FROZEN if getattr(r, "xc_frozen", False) else 0), r.dt)
         dims = _Dims(len(self.groups), len(self.runs), PRECISIONS[precision], self.n_t, 1 if per_l else 0)
         ctx = ctypes.c_void_p()
         self._check(self.lib.ggb_create(ctypes.byref(dims), gd, rd, ctypes.byref(ctx)), None)

@@ -41,6 +41,7 @@ class RunInputs:
     use_hartree: int = 1
     target_id: int = 0
     xc_correlation: bool = False
+    xc_frozen: bool = False        # exchange-correlation potential held at its t = 0 value
     name: str = ""
     omega0: float = 0.057
     angular: str = "reference"     # "reference": the FF/FP/D/P/S chain; "theta": one phase at the P nodes
@@ -79,7 +80,7 @@ def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.
               mask_width: Optional[float] = None, n_har: int = 4, use_hartree: int = 1,
               target_id: int = 0, xc_correlation: bool = False, name: str = "",
               omega0: float = 0.057, device: Optional[str] = None,
-              W: Optional[np.ndarray] = None, angular: str = "reference") -> RunInputs:
+              W: Optional[np.ndarray] = None, angular: str = "reference", xc_frozen: bool = False) -> RunInputs:
     """Assemble one run.
 
     absorber = "cap":  the reference's Manolopoulos CAP starting at ``cap_r_mask``, entering the
@@ -117,7 +118,7 @@ def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.
         occ=np.array([o.occ for o in gs.orbitals], dtype=np.int32),
         rho_frozen=gs.rho_frozen.copy(), E=np.ascontiguousarray(E, dtype=np.float64),
         n_har=n_har, use_hartree=use_hartree, target_id=target_id,
-        xc_correlation=xc_correlation, name=name, omega0=omega0, angular=angular)
+        xc_correlation=xc_correlation, name=name, omega0=omega0, angular=angular, xc_frozen=xc_frozen)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -172,6 +173,12 @@ def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H",
 # benchmark configurations
 # ----------------------------------------------------------------------------------------------
 
+# Angular step of the benchmark configurations: "theta" (one phase per half-step at the Gauss nodes,
+# the form these configurations are benchmarked in) or "reference" (the reference's FF/FP/D/P/S chain,
+# the parity form).  The reference_like() runs always use the reference's chain.
+BENCH_ANGULAR = "reference"
+
+
 @dataclasses.dataclass
 class LaserSpec:
     intensity: float      # W/cm^2
@@ -207,7 +214,8 @@ ATOMS = {
 def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser: LaserSpec,
                  mask_width: float, zeta: float = 0.5, n_steps: Optional[int] = None,
                  device: Optional[str] = None, gs_cache: Optional[dict] = None,
-                 W: Optional[np.ndarray] = None, angular: str = "reference") -> RunInputs:
+                 W: Optional[np.ndarray] = None, angular: Optional[str] = None,
+                 n_har: Optional[int] = None, xc_frozen: bool = False) -> RunInputs:
     """One of the benchmark configurations: sin^2 pulse, cos^(1/8) mask, Z = true nuclear charge.
 
     Hartree/XC runs use the reference's multipole treatment (L <= 3, N_har = 4) with Slater
@@ -226,29 +234,33 @@ def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser
     n_t = full if n_steps is None else n_steps
     E = I.field_sin2(n_t, dt, laser.e0, laser.omega, laser.cycles, laser.cep)
     target = 0 if not spec.interacting else 1
+    if n_har is None:
+        n_har = 4 if spec.interacting else 2
     return build_run(grid, l_max + 1, dt, gs, E, absorber="mask", mask_width=mask_width,
-                     n_har=4 if spec.interacting else 2, use_hartree=1 if spec.interacting else 0,
+                     n_har=n_har, use_hartree=1 if spec.interacting else 0,
                      target_id=target, xc_correlation=spec.correlation,
                      name=f"{atom}-N{n_r}-L{l_max}", omega0=laser.omega, device=device, W=W,
-                     angular=angular)
+                     angular=BENCH_ANGULAR if angular is None else angular, xc_frozen=xc_frozen)
 
 
-def config_hydrogen(n_steps=None, device=None) -> RunInputs:
+def config_hydrogen(n_steps=None, device=None, angular=None) -> RunInputs:
     """H FP64: N_r=200, r_max=100, l_max=32, 800 nm, 1e14 W/cm^2, 4-cycle sin^2, dt=0.05, mask 20 a.u."""
     return baseline_run("H", 200, 100.0, 32, 0.05, LaserSpec(1e14, 800.0, 4.0, 0.0), 20.0,
-                        n_steps=n_steps, device=device)
+                        n_steps=n_steps, device=device, angular=angular)
 
 
-def config_helium(n_steps=None, device=None) -> RunInputs:
-    """He LDA FP64: N_r=400, r_max=200, l_max=64, 800 nm, 1.5e14, 8 cycles, dt=0.03, mask 40 a.u."""
+def config_helium(n_steps=None, device=None, angular=None) -> RunInputs:
+    """He LDA FP64: N_r=400, r_max=200, l_max=64, 800 nm, 1.5e14, 8 cycles, dt=0.03, mask 40 a.u.;
+    in the theta form the Hartree potential of every multipole L = 0 .. 2 l_max = 128."""
+    a = BENCH_ANGULAR if angular is None else angular
     return baseline_run("He", 400, 200.0, 64, 0.03, LaserSpec(1.5e14, 800.0, 8.0, 0.0), 40.0,
-                        n_steps=n_steps, device=device)
+                        n_steps=n_steps, device=device, angular=a, n_har=129 if a == "theta" else 4)
 
 
-def config_argon(n_steps=None, device=None) -> RunInputs:
+def config_argon(n_steps=None, device=None, angular=None, xc_frozen=False) -> RunInputs:
     """Ar LDA: N_r=600, r_max=300, l_max=96, 800 nm, 1.4e14, 10 cycles, dt=0.02, mask 60 a.u."""
     return baseline_run("Ar", 600, 300.0, 96, 0.02, LaserSpec(1.4e14, 800.0, 10.0, 0.0), 60.0,
-                        n_steps=n_steps, device=device)
+                        n_steps=n_steps, device=device, angular=angular, xc_frozen=xc_frozen)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -326,9 +338,10 @@ def hhe_draws(n_runs: int = 256, seed: int = 0, ladder: Sequence[GridRung] = HHE
 
 
 def argon_ensemble(n_runs: int = 64, seed: int = 0, n_steps: Optional[int] = None, device=None,
-                   ladder: Sequence[GridRung] = ARGON_LADDER, only=None) -> List[RunInputs]:
-    """The runs of ``argon_draws``."""
-    return _ensemble(argon_draws(n_runs, seed, ladder), n_steps, device, only=only)
+                   ladder: Sequence[GridRung] = ARGON_LADDER, only=None, xc_frozen: bool = False) -> List[RunInputs]:
+    """The runs of ``argon_draws``; ``xc_frozen`` keeps each run's exchange-correlation potential at its
+    ground-state value (the Hartree multipoles still follow the density)."""
+    return _ensemble(argon_draws(n_runs, seed, ladder), n_steps, device, only=only, xc_frozen=xc_frozen)
 
 
 def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None, device=None,
@@ -337,7 +350,7 @@ def hhe_ensemble(n_runs: int = 256, seed: int = 0, n_steps: Optional[int] = None
     return _ensemble(hhe_draws(n_runs, seed, ladder), n_steps, device, only=only)
 
 
-def _ensemble(dr: EnsembleDraws, n_steps, device, only=None):
+def _ensemble(dr: EnsembleDraws, n_steps, device, only=None, xc_frozen: bool = False):
     """The runs of an ensemble from its drawn parameters; ``only`` = indices of the runs to build
     (the draws are made for the whole ensemble first, so a selected run equals its twin in the full
     ensemble)."""
@@ -353,7 +366,7 @@ def _ensemble(dr: EnsembleDraws, n_steps, device, only=None):
         laser = LaserSpec(float(I0[i]), float(lam[i]), cycles, float(cep[i]))
         key = (a, g.n_r, g.r_max, g.l_max)
         run = baseline_run(a, g.n_r, g.r_max, g.l_max, dt, laser, 0.2 * g.r_max, n_steps=n_steps,
-                           device=device, gs_cache=gs_cache, W=w_cache.get(key))
+                           device=device, gs_cache=gs_cache, W=w_cache.get(key), xc_frozen=xc_frozen)
         w_cache[key] = run.W
         run.name = f"{a}-{i}-N{g.n_r}-L{g.l_max}"
         runs.append(run)

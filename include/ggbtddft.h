@@ -45,7 +45,7 @@ enum { GGB_COUPLING_P = 0, GGB_COUPLING_FP = 1, GGB_COUPLING_D = 2, GGB_COUPLING
 /* run flags */
 enum {
   GGB_RUN_XC_PW92 = 1,  /* add PW92 correlation to the TD exchange potential (not in the reference) */
-  GGB_RUN_THETA = 2     /* theta form (not in the reference): each angular half-step is one diagonal
+  GGB_RUN_THETA = 2,    /* theta form (not in the reference): each angular half-step is one diagonal
                            phase at the Gauss nodes x_j of the P coupling (its eigenbasis, the V/D of
                            coupling P), exp(-i dt/2 [r E x_j + sum_{L=1}^{n_har-1} v_L(r) P_L(x_j)
                            + dv_0(r) + dv_xc(r)]), instead of the reference's FF/FP/D/P/S chain: two
@@ -53,6 +53,11 @@ enum {
                            4 < n_har <= 2 l_max + 1: every multipole by exact Gauss-Legendre
                            quadrature of the density on 2 N_l nodes.  Runs of a group share it; the
                            split_int8 and FP64 forms only. */
+  GGB_RUN_XC_FROZEN = 4 /* keep the exchange(-correlation) potential at its t = 0 value (the Hartree
+                           multipoles still follow the density); not in the reference.  With the
+                           adiabatic exchange following the monopole density, all-electron argon is
+                           unstable in field-free propagation (a 1e-10 perturbation grows with an
+                           e-folding time of ~0.5 a.u.); with it frozen it is not. */
 };
 
 /* error codes */

@@ -19,7 +19,9 @@ sm_100a from the reference's own sources by ``oracle/build_ref.py``) on identica
 the resulting dipole files are committed as golden fixtures under ``tests/golden/``.
 
 Options beyond the reference (off by default, so the default reproduces the reference):
-``xc_correlation`` (adds PW92 correlation to the TD exchange potential), the ``norm`` output, and
+``xc_correlation`` (adds PW92 correlation to the TD exchange potential), ``xc_frozen`` (keeps the
+exchange(-correlation) potential at its t = 0 value while the Hartree multipoles follow the density),
+the ``norm`` output, and
 ``angular = "theta"``: the angular half-step as one diagonal phase at the Gauss nodes of the dipole
 coupling (the eigenbasis of the reference's P coupling, couplingP.cuh:1-125), holding the laser term
 and the Hartree potential of the multipoles L = 0 .. n_har - 1 (n_har up to 2 l_max + 1) with the
@@ -126,6 +128,7 @@ class OracleProblem:
     target_id: int = 0
     # options beyond the reference (defaults reproduce it)
     xc_correlation: bool = False
+    xc_frozen: bool = False          # exchange(-correlation) potential held at its t = 0 value
     angular: str = "reference"      # "reference" | "theta"
 
     @property
@@ -386,6 +389,8 @@ class OracleState:
     def exchange(self, rho0, clamp):
         """d_exchangePotential[0] (h_calculateExchangeCorrelationPotential.cuh:1-45)."""
         p = self.p
+        if clamp and p.xc_frozen:
+            return self.vexc0.copy()
         dens = p.n_g * (p.n_g + 1) / 2.0 * (rho0 / 4.0 / np.pi + p.rho_frozen) / p.drdx * np.power(p.P, 2.0)
         if clamp:
             dens = np.maximum(dens, 0.0)

@@ -14,7 +14,7 @@ def to_oracle(run: P.RunInputs) -> OracleProblem:
     return OracleProblem(r=run.grid.r, drdx=run.grid.drdx, P=run.grid.P, W=run.W, V=run.V, D=run.D,
                          x0=run.x0, m=run.m_active, occ=run.occ, rho_frozen=run.rho_frozen, E=run.E,
                          dt=run.dt, n_har=run.n_har, use_hartree=run.use_hartree, target_id=run.target_id,
-                         xc_correlation=run.xc_correlation, angular=run.angular)
+                         xc_correlation=run.xc_correlation, xc_frozen=run.xc_frozen, angular=run.angular)
 
 
 def load_ref_case(name):

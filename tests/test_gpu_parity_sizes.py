@@ -185,3 +185,11 @@ def test_int8_theta_form_every_multipole_tracks_the_oracle():
     assert st == 0, msg
     assert rel_err(got["norm"], ref["norm"]) < TOL_I8
     assert rel_err(got["dipole"].sum(axis=0), ref["dipole"].sum(axis=0)) < TOL_I8
+
+
+@pytest.mark.parametrize("angular", ["reference", "theta"])
+def test_fp64_frozen_xc_matches_the_oracle(angular):
+    """GGB_RUN_XC_FROZEN: the exchange-correlation potential stays at its t = 0 value."""
+    run = P.reference_like(45, 9, 20, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=3)
+    run = dataclasses.replace(run, xc_frozen=True, angular=angular)
+    _fp64_vs_oracle(run, 20)

@@ -95,3 +95,31 @@ def test_density_multipoles_equal_the_literal_loops(n_l, ms):
     a = st.density_multipoles_literal(x)
     b = st.density_multipoles(x)
     assert np.abs(a - b).max() <= 1e-14 * np.abs(a).max()
+
+
+def test_argon_exchange_feedback_amplifies_perturbations_and_frozen_xc_does_not():
+    """All-electron argon in the adiabatic LDA exchange of the reference (Slater exchange of the
+    monopole density, h_calculateExchangeCorrelationPotential.cuh:26-45) is unstable in field-free
+    propagation: a 1e-10 perturbation of the self-consistent ground state grows by ~1e7 in 400 steps
+    (8 a.u.).  With the exchange-correlation potential held at its ground-state value (the Hartree
+    multipoles still follow the density) it stays at the size of the perturbation.  This is why no
+    arithmetic other than the identical FP64 sequence can reproduce the argon LDA spectrum, and why
+    the argon benchmark can freeze xc."""
+    import numpy as np
+    from ggbtddft_b200 import accuracy as A
+    from ggbtddft_b200 import problems as P
+    from oracle.step_oracle import OracleState
+    grown = {}
+    for frozen in (False, True):
+        run = P.baseline_run("Ar", 100, 50.0, 8, 0.02, P.LaserSpec(1.4e14, 800.0, 10.0, 0.0), 10.0,
+                             n_steps=400, xc_frozen=frozen).with_field(np.zeros(400))
+        a = OracleState(to_oracle(run))
+        b = OracleState(to_oracle(A.perturb_orbitals(run, 1e-10)))
+        a.init_potentials()
+        b.init_potentials()
+        for t in range(400):
+            a.step(t)
+            b.step(t)
+        grown[frozen] = np.abs(a.x - b.x).max() / np.abs(a.x).max()
+    assert grown[False] > 1e-5, grown          # > 1e5-fold growth with the exchange following the density
+    assert grown[True] < 1e-7, grown           # < 1e3-fold with it frozen
