@@ -39,9 +39,23 @@ import numpy as np  # noqa: E402
 # workloads
 # ---------------------------------------------------------------------------------------------
 
-def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8", only=None):
+def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8", only=None,
+                  angular: str = "theta", xc_frozen: bool = False):
     """Return (runs, precision, description dict); ``split`` is the form of the non-FP64 workloads;
-    ``only`` builds just those runs of an ensemble workload (the CPU sample needs one)."""
+    ``only`` builds just those runs of an ensemble workload (the CPU sample needs one); ``angular``
+    and ``xc_frozen`` set every run's angular step and exchange-correlation treatment."""
+    runs, precision, desc = _workload_runs(name, n_t, device, split, only)
+    import dataclasses
+    runs = [dataclasses.replace(r, angular=angular, xc_frozen=xc_frozen or r.xc_frozen) for r in runs]
+    if runs and any(r.n_har > 4 for r in runs) and angular != "theta":
+        runs = [dataclasses.replace(r, n_har=4) for r in runs]
+    desc = dict(desc, angular=angular + (" (one phase per half-step at the P coupling's Gauss nodes)"
+                                         if angular == "theta" else " (the reference's FF/FP/D/P/S chain)"),
+                xc="frozen at the ground state" if xc_frozen else "adiabatic (follows the density)")
+    return runs, precision, desc
+
+
+def _workload_runs(name: str, n_t: int, device=None, split: str = "split_int8", only=None):
     from ggbtddft_b200 import problems as P
     if name.startswith("ar-ens64"):
         precision = "fp64" if name.endswith("fp64") else split
@@ -86,7 +100,7 @@ def workload_runs(name: str, n_t: int, device=None, split: str = "split_int8", o
                                             "800 nm 1.4e14 W/cm^2 10-cycle sin^2 (first steps of the pulse)",
                                    runs=1, n_r=600, l_max=96, n_orb=9, precision="fp64")
     if name == "he-fp64":
-        run = P.config_helium(n_steps=n_t, device=device)
+        run = P.config_helium(n_steps=n_t, device=device, angular="theta")
         return [run], "fp64", dict(workload="He LDA, 1 orbital, N_r=400, r_max=200, l_max=64, dt=0.03",
                                    runs=1, n_r=400, l_max=64, n_orb=1, precision="fp64")
     if name == "h-fp64":
@@ -112,6 +126,8 @@ def workload_groups(name: str):
 
 
 DEFAULT_WORKLOAD = "ar-ens64"
+DEFAULT_ANGULAR = "reference"
+DEFAULT_XC_FROZEN = 0
 # tensor-core products executed per algorithmic real product, and the peak they run against
 SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (BF16)
                   "split_int8": 10}   # int8 slice pairs (j, m), 0-based, with j + m <= 3
@@ -274,7 +290,8 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     n_t = args.warmup + args.steps + 8
-    runs, precision, desc = workload_runs(args.workload, n_t, device="cuda", split=args.precision)
+    runs, precision, desc = workload_runs(args.workload, n_t, device="cuda", split=args.precision,
+                                          angular=args.angular, xc_frozen=args.xc_frozen)
     units_per_step = sum(r.n_orb for r in runs)
     tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
     stream = torch.cuda.Stream()
@@ -428,7 +445,9 @@ def run_ours(args, rank, world, dist):
                 e2e=None if e2e_value is None else dict(
                     value=e2e_value, unit="orbital-steps/s", h2d_bytes_per_step=int(h2d / args.steps),
                     d2h_bytes_per_step=int(d2h / args.steps)),
-                gpu_launches=LAUNCHES_PER_GROUP_STEP[precision] * args.steps * len(tp.groups),
+                gpu_launches=args.steps * sum(LAUNCHES_PER_GROUP_STEP[precision] +
+                                              (4 if runs[m[0]].angular == "theta" and runs[m[0]].n_har > 4
+                                               and runs[m[0]].use_hartree else 0) for m in tp.groups),
                 fp64_per_instance=fp64_inst)
 
 
@@ -451,14 +470,14 @@ def cpu_port_rate(runs, n_steps: int, warmup: int = 1):
     return r.n_orb * n_steps / dt, dt
 
 
-def cpu_workload_rate(name: str, n_steps: int, warmup: int):
+def cpu_workload_rate(name: str, n_steps: int, warmup: int, angular: str = "theta", xc_frozen: bool = False):
     """The CPU oracle on a bounded sample of the workload: one run per grid group, ``n_steps`` timed
     steps each (after ``warmup``), weighted by the runs in its group.  Returns (orbital-steps/s of the
     whole workload, seconds timed, estimated CPU seconds of one whole-workload step, sample text, the
     workload's description)."""
     units, step_s, timed, parts, desc = 0.0, 0.0, 0.0, [], None
     for idx, count, label in workload_groups(name):
-        runs, _, desc = workload_runs(name, n_steps + warmup + 8, only=[idx])
+        runs, _, desc = workload_runs(name, n_steps + warmup + 8, only=[idx], angular=angular, xc_frozen=xc_frozen)
         runs = runs[:1] if idx == 0 else runs
         rate, sec = cpu_port_rate(runs, n_steps, warmup)
         per_step = sec / n_steps
@@ -482,7 +501,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     n, w = min(args.steps, REF_SAMPLE_STEPS), min(args.warmup, 2)
-    rate, timed, step_s, text, desc = cpu_workload_rate(args.workload, n, w)
+    rate, timed, step_s, text, desc = cpu_workload_rate(args.workload, n, w, args.angular, args.xc_frozen)
     return dict(value=rate, desc=desc, seconds=timed, step_seconds=step_s, steps_timed=n, sample=text)
 
 
@@ -499,6 +518,11 @@ def main():
                     help="form of the split-precision workloads (FP64 workloads end in -fp64)")
     ap.add_argument("--cpu-sample-steps", type=int, default=4,
                     help="oracle steps timed per grid group for cpu_baseline (0: skip)")
+    ap.add_argument("--angular", default=DEFAULT_ANGULAR, choices=["reference", "theta"],
+                    help="angular step of every run: theta (one phase per half-step at the Gauss nodes) or the "
+                         "reference's coupling chain")
+    ap.add_argument("--xc-frozen", type=int, default=DEFAULT_XC_FROZEN,
+                    help="1: exchange-correlation potential held at its ground-state value")
     ap.add_argument("--clocks-csv", default=None,
                     help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")
@@ -534,7 +558,8 @@ def main():
     res = run_ours(args, rank, world, dist)
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_steps > 0:
-        rate, timed, _, text, _ = cpu_workload_rate(args.workload, args.cpu_sample_steps, 1)
+        rate, timed, _, text, _ = cpu_workload_rate(args.workload, args.cpu_sample_steps, 1, args.angular,
+                                                    args.xc_frozen)
         cpu = dict(value=rate, unit="orbital-steps/s", cores=cores, kind="port", sample=f"{text}; {timed:.1f} s timed")
     if rank == 0:
         desc = dict(res["desc"])

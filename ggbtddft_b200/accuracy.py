@@ -278,6 +278,45 @@ def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed:
                 norm_drift_max=max(q["norm_drift_max"] for q in per))
 
 
+def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64, seed: int = 0,
+                                angular: str = "theta", xc_frozen: bool = True, per_rung: int = 1) -> dict:
+    """Whole pulses of the argon focal scan: all runs batched in ``precision`` (one context, grid groups
+    on concurrent streams, each run followed by zero field up to the longest pulse) against the FP64
+    form of ``per_rung`` runs per grid rung, each stepped alone over its own pulse.  Per checked
+    instance: the largest relative error of the harmonic intensities up to its cutoff (total dipole
+    summed over every l), the dipole L2 difference and the norm difference."""
+    dr = P.argon_draws(n_runs, seed)
+    runs = P.argon_ensemble(n_runs, seed=seed, device="cuda", xc_frozen=xc_frozen)
+    runs = [dataclasses.replace(r, angular=angular) for r in runs]
+    n = max(r.n_t for r in runs)
+    tst, t_tst, st_tst = _batched_totals(runs, precision, n)
+    checked = [i for members in dr.grid_groups().values() for i in members[:per_rung]]
+    per = []
+    t_ref = 0.0
+    for i in checked:
+        r = runs[i]
+        ref, t1, st1 = _batched_totals([r], "fp64", r.n_t)
+        t_ref += t1
+        m = r.n_t
+        d_r, d_t = ref[0]["dipole"][:m], tst[i]["dipole"][:m]
+        w, s_r = S.hhg_spectrum(d_r, r.dt)
+        _, s_t = S.hhg_spectrum(d_t, r.dt)
+        q_cut = S.cutoff_order(IONISATION_POTENTIAL["Ar"], float(np.abs(r.E).max()), r.omega0)
+        herr = S.harmonic_errors(s_t, s_r, w, r.omega0, q_cut)
+        per.append(dict(run=i, n_r=r.n_r, l_max=r.n_l - 1, steps=m, cutoff_order=q_cut, fp64_status=st1[0],
+                        harmonic_rel_err_max=float(herr.max()), harmonic_rel_err=herr.tolist(),
+                        dipole_rel_l2=float(np.linalg.norm(d_t - d_r) / np.linalg.norm(d_r)),
+                        norm_drift_max=float(np.abs(tst[i]["norm"][:, :m] - ref[0]["norm"][:, :m]).max())))
+    return dict(config=f"argon focal scan, {n_runs} runs (seed {seed}), whole pulses, angular {angular}, "
+                       f"xc {'frozen at the ground state' if xc_frozen else 'adiabatic'}",
+                precision=precision, steps_stepped=n, seconds=dict(batched=t_tst, fp64_checked=t_ref),
+                batched_status=st_tst, per_instance=per,
+                harmonic_rel_err_max=max(q["harmonic_rel_err_max"] for q in per),
+                instances_within_1e3=int(sum(q["harmonic_rel_err_max"] <= 1e-3 for q in per)),
+                dipole_rel_l2_max=max(q["dipole_rel_l2"] for q in per),
+                norm_drift_max=max(q["norm_drift_max"] for q in per))
+
+
 CONFIGS = {
     "hydrogen": ("H", P.config_hydrogen),
     "helium": ("He", P.config_helium),
@@ -300,10 +339,21 @@ def main(argv=None):
     ap.add_argument("--hhe-ensemble", action="store_true",
                     help="instead: the 256-run H/He ensemble over whole pulses, batched, against batched FP64")
     ap.add_argument("--angular", default="reference", choices=["reference", "theta"])
+    ap.add_argument("--argon-ensemble-full", action="store_true",
+                    help="instead: whole pulses of the 64-run argon ensemble, batched, against FP64 runs of "
+                         "one run per grid rung")
+    ap.add_argument("--xc-frozen", action="store_true", help="exchange-correlation held at the ground state")
     ap.add_argument("--sweep", action="store_true",
                     help="instead: FP64 self-sensitivity of argon LDA for dt in {0.02, 0.01, 0.005} and N_har "
                          "in {2, 3, 4} over the whole pulse")
     args = ap.parse_args(argv)
+    if args.argon_ensemble_full:
+        rep = compare_argon_ensemble_full(args.precision, angular=args.angular, xc_frozen=args.xc_frozen)
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(rep) + "\n")
+        print(json.dumps({k: v for k, v in rep.items() if k != "per_instance"}))
+        return
     if args.hhe_ensemble:
         rep = compare_hhe_ensemble(args.precision, angular=args.angular)
         if args.out:
@@ -327,6 +377,10 @@ def main(argv=None):
         return
     atom, builder = CONFIGS[args.config]
     run = builder(n_steps=args.steps, device="cuda")
+    if args.angular != "reference":
+        run = dataclasses.replace(run, angular=args.angular, n_har=129 if atom == "He" else run.n_har)
+    if args.xc_frozen:
+        run = dataclasses.replace(run, xc_frozen=True, name=run.name + "-xcfrozen")
     if args.frozen:
         run = dataclasses.replace(run, use_hartree=0, name=run.name + "-frozen")
     rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity)
