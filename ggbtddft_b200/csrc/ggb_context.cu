@@ -529,10 +529,11 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     g.V.assign(4, std::vector<std::vector<double>>(g.d.n_m));
     g.D.assign(4, std::vector<std::vector<double>>(g.d.n_m));
     g.ang_set.assign(4, std::vector<bool>(g.d.n_m, false));
-    // observables partials: one per CTA tile of radii.  The FP64 form's angular kernel takes 16
-    // radii per CTA (twice the CTAs of a 32-radius tile: a single run fills the GPU better); the
-    // int8 form's takes 32, or 16 when N_l > 128 (two M tiles of channels)
-    g.obs_seg = (dims->precision == GGB_FP64 || (dims->precision == GGB_SPLIT_INT8 && g.d.n_l > 128)) ? 16 : TR;
+    // observables partials: one per CTA tile of radii.  The angular kernels take 32 radii per CTA
+    // (each CTA streams the chain matrices once per product: fewer radii per CTA cost more of that
+    // traffic than the extra CTAs gain, measured for the FP64 form), the int8 form 16 when N_l > 128
+    // (two M tiles of channels)
+    g.obs_seg = (dims->precision == GGB_SPLIT_INT8 && g.d.n_l > 128) ? 16 : TR;
     g.n_tiles = (g.d.n_r + g.obs_seg - 1) / g.obs_seg;
     g.ldS = ((g.d.n_l + 7) / 8) * 8;
   }

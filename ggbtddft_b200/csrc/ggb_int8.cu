@@ -484,7 +484,7 @@ __device__ __forceinline__ void slice_put(uint8_t* xb, int p, int k, double2 v, 
 // exponent serves the whole chain.  The chain matrices S^T stream through a TMA pipeline, one
 // slice plane per stage.  Orbitals in and out are complex128 (xout may alias xin: each CTA reads
 // its whole tile before it writes).
-template <int NP, bool SECOND_HALF>
+template <int NP, bool SECOND_HALF, bool THETA>
 __global__ void __launch_bounds__(A8_THREADS, 2)
 k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, const double2* xin, double2* xout) {
   constexpr int NB = 2 * NP;                 // B rows: Re of NP points, then Im
@@ -703,7 +703,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       const double dj = (op.phase != PH_NONE && j >= m && j < n_l) ? Dv[j] : 0.0;
       const int pb = op.phase == PH_P ? 1 : op.phase == PH_D ? 2 : 3;
       // the theta form: angle = pbase1 x_j + pbase2 P_2(x_j) + pbase3 P_3(x_j) + pbase4 (all x dt/2)
-      const bool th = op.phase == PH_THETA && j >= m && j < n_l;
+      const bool th = THETA && op.phase == PH_THETA && j >= m && j < n_l;
       const double p2j = th ? legendre_p2(dj) : 0.0, p3j = th ? legendre_p3(dj) : 0.0;
       const bool post_s = last && !SECOND_HALF && ch.post_s && j < n_l;
       const double pj = post_s ? pco[j] : 0.0;
@@ -741,13 +741,16 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int p = p0 + u;
-          if (th) {
-            double ang = pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p];
-            // n_har > 4: the multipoles L >= 1 at this node come from the exact-quadrature table
-            if (g.theta_tab && r0 + p < g.n_r) ang += run.htab[((size_t)m * n_l + j) * g.n_r + r0 + p] * hdt;
-            v[u] = rotd(v[u], ang);
+          if constexpr (THETA) {
+            if (th) {
+              double ang = pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p];
+              // n_har > 4: the multipoles L >= 1 at this node come from the exact-quadrature table
+              if (g.theta_tab && r0 + p < g.n_r) ang += run.htab[((size_t)m * n_l + j) * g.n_r + r0 + p] * hdt;
+              v[u] = rotd(v[u], ang);
+            }
+          } else {
+            if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
           }
-          else if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
           if (post_s) v[u] = rotd(v[u], pbase[4][p] + pj * pbase[2][p]);
           if (!last) {
             if (j < lk) {
@@ -1064,10 +1067,14 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
     case 32: I8_CK(set_max_dynamic_smem((const void*)k_radial_i8<32>, optin)); q.smem = r8_smem<32>(q.stages); break;
     default: I8_CK(set_max_dynamic_smem((const void*)k_radial_i8<64>, optin)); q.smem = r8_smem<64>(q.stages); break;
   }
-  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, false>, optin));
-  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, true>, optin));
-  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, false>, optin));
-  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, true>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, false, false>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, true, false>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, false, false>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, true, false>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, false, true>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<32, true, true>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, false, true>, optin));
+  I8_CK(set_max_dynamic_smem((const void*)k_angular_i8<16, true, true>, optin));
   I8_CK(cudaDeviceSynchronize());
   return GGB_OK;
 }
@@ -1097,13 +1104,15 @@ void int8_angular(MixedGroup& mg, const GroupArgs& a, int half, const double2* x
   t.n_mats = q.n_mats;
   t.n_var = I8_S_VARIANTS;
   const dim3 grid(a.n_cols * ((a.n_r + q.np - 1) / q.np));
+#define GGB_A8(NP, SH, TH) k_angular_i8<NP, SH, TH><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout)
   if (q.np == 32) {
-    if (half == 0) k_angular_i8<32, false><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout);
-    else k_angular_i8<32, true><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout);
+    if (half == 0) { if (a.theta) GGB_A8(32, false, true); else GGB_A8(32, false, false); }
+    else { if (a.theta) GGB_A8(32, true, true); else GGB_A8(32, true, false); }
   } else {
-    if (half == 0) k_angular_i8<16, false><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout);
-    else k_angular_i8<16, true><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout);
+    if (half == 0) { if (a.theta) GGB_A8(16, false, true); else GGB_A8(16, false, false); }
+    else { if (a.theta) GGB_A8(16, true, true); else GGB_A8(16, true, false); }
   }
+#undef GGB_A8
 }
 
 void int8_slice_x(MixedGroup& mg, const GroupArgs& a, const double2* x, cudaStream_t s) {

@@ -11,7 +11,7 @@
 //                  dipoleAcceleration.cuh:1-71), so the orbitals are read once per half-step.
 //  k_radial_fp64   x_l <- A_l x_l for every l with A_l(a,b) = W[l][b][a]: the batched ZGEMM of
 //                  h_propagationH0 (h_timePropagation.cuh:1-30), out of place.  Persistent, two CTAs
-//                  per SM; a producer warp streams the W rows and x segments of each 32-wide k chunk
+//                  per SM; a producer warp streams the W rows and x segments of each 16-wide k chunk
 //                  into a 3-stage shared-memory ring with cp.async.bulk (mbarrier transaction
 //                  counts), so that ~200 KB per SM are in flight whatever the occupancy; four
 //                  consumer warps (one output radius per thread, TC orbital columns in registers)
@@ -197,9 +197,9 @@ void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, doubl
 // radial propagator, FP64
 // ---------------------------------------------------------------------------------------------
 
-constexpr int RAD_CW = 2;                 // consumer warps: one output radius per thread
+constexpr int RAD_CW = 4;                 // consumer warps: one output radius per thread
 constexpr int RAD_TI = 32 * RAD_CW;       // rows (output radii) per tile
-constexpr int RAD_KC = 32;                // k per stage
+constexpr int RAD_KC = 16;                // k per stage (3 stages of ~35 KB: two CTAs per SM)
 constexpr int RAD_STAGES = 3;
 constexpr int RAD_THREADS = 32 * (RAD_CW + 1);
 
