@@ -150,6 +150,18 @@ def read_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def reference_binary_record():
+    """The reference's own main.cu timed on a B200 (a committed record of oracle/time_ref.py's run;
+    nothing under oracle/ is executed here)."""
+    p = os.path.join(ROOT, "profiles", "reference_main_cu__ar9_n608_l96.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return dict(value=d["orbital_steps_per_s"], unit="orbital-steps/s", ms_per_step=d["ms_per_step"],
+                config=f"argon, {d['n_kso']} orbitals, N_r {d['n_r']}, N_l {d['n_l']}, {d['n_t']} steps",
+                how=d["how"] + "; recorded in profiles/reference_main_cu__ar9_n608_l96.json")
+
+
 def compute_peaks(stream_handle):
     """FP64 FMA and tcgen05 int8 peaks of this GPU from the library's own microbenchmarks
     (ggb_measure_peaks), taken once before the timed region."""
@@ -570,7 +582,8 @@ def main():
                     scaling="weak", vs_baseline=None, dtype={"fp64": "f64", "split_bf16": "f32+split-bf16", "split_int8": "f64+split-int8"}[res["precision"]],
                     data="synthetic (seeded laser parameters; LDA ground state computed at set-up)", config=desc,
                     roofline=res["roofline"], cpu_baseline=cpu, e2e=res["e2e"], clocks=res["clocks"],
-                    gpu_launches=res["gpu_launches"], fp64_per_instance=res["fp64_per_instance"])
+                    gpu_launches=res["gpu_launches"], fp64_per_instance=res["fp64_per_instance"],
+                    reference_main_cu_b200=reference_binary_record())
         print(json.dumps(line))
     if dist:
         torch.distributed.destroy_process_group()
