@@ -204,18 +204,22 @@ def radial_propagators(grid: RadialGrid, n_l: int, dt: float, v0: np.ndarray, vs
         eye = torch.eye(n_r, dtype=torch.complex128, device=dev)
         base = torch.from_numpy(np.asarray(v0 + vscf - 1j * mask_r, dtype=np.complex128)).to(dev)
         rm = None if row_mask is None else torch.from_numpy(row_mask).to(dev, torch.complex128)
-        for l in range(n_l):
-            if l > 256 or method != "CN":
-                H = torch.from_numpy(radial_hamiltonian(grid, l, v0, vscf, mask_r)).to(dev)
-                out[l] = _propagator_from_h(H.cpu().numpy(), dt, method, l, grid.r, row_mask)
-                continue
-            H = -0.5 * T + torch.diag(base + l * (l + 1) / 2.0 / r ** 2)
-            Wm = eye - 0.5j * dt * H
-            Wp = eye + 0.5j * dt * H
-            W = torch.linalg.solve(Wp, Wm)
+        cn = [l for l in range(n_l) if l <= 256 and method == "CN"]
+        # Crank-Nicolson for every l at once: a batch of N_r x N_r complex128 solves on the device,
+        # in chunks that keep ~2 GB of matrices per solve
+        chunk = max(1, int(2e9 // (3 * 16 * n_r * n_r)))
+        for c0 in range(0, len(cn), chunk):
+            ls = torch.tensor(cn[c0:c0 + chunk], dtype=torch.float64, device=dev)
+            diag = base[None, :] + (ls * (ls + 1.0) / 2.0)[:, None] / (r ** 2)[None, :]
+            H = -0.5 * T[None] + torch.diag_embed(diag)
+            W = torch.linalg.solve(eye[None] + 0.5j * dt * H, eye[None] - 0.5j * dt * H)
             if rm is not None:
-                W = rm[:, None] * W
-            out[l] = W.cpu().numpy()
+                W = rm[None, :, None] * W
+            out[cn[c0]:cn[c0] + len(ls)] = W.cpu().numpy()
+        for l in range(n_l):
+            if l not in cn:
+                out[l] = _propagator_from_h(radial_hamiltonian(grid, l, v0, vscf, mask_r), dt, method, l,
+                                            grid.r, row_mask)
         return out
     for l in range(n_l):
         H = radial_hamiltonian(grid, l, v0, vscf, mask_r)
@@ -373,6 +377,34 @@ def angular_eigensystems(n_l: int, n_m: int) -> Dict[str, Tuple[np.ndarray, np.n
             V[m, m:, m:] = v
         V.setflags(write=False)
         D.setflags(write=False)
+        out[c] = (V, D)
+    return out
+
+
+def angular_eigensystems_device(n_l: int, n_m: int, device: str = "cuda") -> Dict[str, Tuple[np.ndarray, np.ndarray]]:
+    """The same eigensystems with torch.linalg.eigh on ``device`` (FP64), every m of a coupling in one
+    batched call: the m blocks l, j >= m are embedded in N_l x N_l matrices whose rows and columns below
+    m carry distinct eigenvalues far outside [-1, 1] (2 + index), so that the m block's eigenpairs are the
+    N_l - m eigenpairs inside [-1, 1]."""
+    import torch
+    dev = torch.device(device)
+    out = {}
+    for c in COUPLINGS:
+        mats = np.zeros((n_m, n_l, n_l))
+        for m in range(n_m):
+            mats[m] = coupling_matrix(c, n_l, m)
+            mats[m, :m, :] = 0.0
+            mats[m, :, :m] = 0.0
+            for k in range(m):
+                mats[m, k, k] = 2.0 + k
+        d, v = torch.linalg.eigh(torch.from_numpy(mats).to(dev))
+        d, v = d.cpu().numpy(), v.cpu().numpy()
+        V = np.zeros((n_m, n_l, n_l))
+        D = np.zeros((n_m, n_l))
+        for m in range(n_m):
+            keep = np.argsort(d[m])[:n_l - m]          # the eigenvalues inside [-1, 1], ascending
+            D[m, m:] = d[m][keep]
+            V[m, m:, m:] = v[m][m:, keep]
         out[c] = (V, D)
     return out
 

@@ -1,0 +1,32 @@
+"""Inputs built on the GPU (FP64, torch.linalg) against the CPU builds that are pinned to the
+reference's internal.py (tests/test_inputs_vs_reference.py)."""
+import numpy as np
+import pytest
+
+from ggbtddft_b200 import inputs as I
+
+pytestmark = pytest.mark.gpu
+
+
+def test_radial_propagators_built_on_the_gpu_equal_the_cpu_build():
+    g = I.make_grid(300, 150.0, I.zeta_physical_to_ref(0.5, 150.0))
+    v0 = -2.0 / g.r
+    vscf = 1.2 * np.exp(-0.7 * g.r) / (1.0 + g.r)
+    mask = I.mask_cos8(g.r, 150.0, 30.0)
+    a = I.radial_propagators(g, 40, 0.03, v0, vscf, np.zeros_like(g.r), row_mask=mask)
+    b = I.radial_propagators(g, 40, 0.03, v0, vscf, np.zeros_like(g.r), row_mask=mask, device="cuda")
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("n_l,n_m", [(33, 1), (97, 2), (161, 3)])
+def test_angular_eigensystems_built_on_the_gpu_equal_the_cpu_build(n_l, n_m):
+    cpu = I.angular_eigensystems(n_l, n_m)
+    gpu = I.angular_eigensystems_device(n_l, n_m, "cuda")
+    for c in I.COUPLINGS:
+        (V, D), (Vg, Dg) = cpu[c], gpu[c]
+        for m in range(n_m):
+            assert np.abs(np.sort(D[m, m:]) - np.sort(Dg[m, m:])).max() < 1e-13
+            for a in (0.3, 2.2):
+                U = V[m] @ np.diag(np.exp(-1j * a * D[m])) @ V[m].T
+                Ug = Vg[m] @ np.diag(np.exp(-1j * a * Dg[m])) @ Vg[m].T
+                assert np.abs((U - Ug)[m:, m:]).max() < 1e-12, (c, m)
