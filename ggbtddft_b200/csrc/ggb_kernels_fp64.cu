@@ -20,6 +20,8 @@
 //                  (occupation-weighted sum over orbitals), Hartree potentials by compensated
 //                  prefix scans (h_calculateHartreePotential.cuh:1-136), LDA exchange
 //                  (h_calculateExchangeCorrelationPotential.cuh:1-56), step counter.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cstdio>
 #include "ggb_internal.cuh"
@@ -37,19 +39,27 @@ constexpr int ANG_JB = 8;   // eigen-channels j per register block
 
 // RT radii per CTA (32, or 16 with the two half-warps on different eigen-channel blocks): lane % RT is
 // the radius, lane / RT picks the half; the group's observables partials cover RT radii each.
-template <int RT>
+// CL = 2: a cluster of two CTAs shares one tile: each computes half of the eigen-channels of every
+// product (reading half of the chain matrix) and writes its half into both CTAs' shared memory
+// (distributed shared memory), a cluster barrier between products; the same arithmetic as CL = 1,
+// with twice the CTAs for runs too small to fill the GPU.
+template <int RT, int CL>
 __global__ void __launch_bounds__(ANG_WARPS * 32)
 k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* __restrict__ xout, int do_obs) {
+  namespace cg = cooperative_groups;
   constexpr int SUB = 32 / RT;                    // lanes groups per warp (1 or 2)
-  constexpr int NSUB = ANG_WARPS * SUB;           // thread groups that stride l and j
+  constexpr int NSUB = ANG_WARPS * SUB;           // thread groups that stride l and j in one CTA
   extern __shared__ double2 sm[];  // two [N_l][RT] buffers
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int lr = lane % RT;                       // radius of this lane
   const int sub = warp * SUB + lane / RT;         // this thread's group
+  const int crank = CL == 2 ? (int)cg::this_cluster().block_rank() : 0;
+  const int gsub = crank * NSUB + sub;            // this thread's group across the cluster
   const int tilesN = (g.n_r + RT - 1) / RT;
-  const int col = blockIdx.x / tilesN;
-  const int tile = blockIdx.x - col * tilesN;
+  const int bt = blockIdx.x / CL;                 // the tile of this CTA (or CTA pair)
+  const int col = bt / tilesN;
+  const int tile = bt - col * tilesN;
   const int r = tile * RT + lr;
   const bool rv = r < g.n_r;
   const int n_l = g.n_l;
@@ -77,7 +87,8 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
   }
   const double hdt = 0.5 * g.dt;
   const double* pco = g.coef + ((size_t)CF_P * g.n_m + m) * n_l;
-  __syncthreads();
+  if constexpr (CL == 2) cg::this_cluster().sync();   // both CTAs running before any remote write
+  else __syncthreads();
 
   const Chain& ch = g.chain[half];
   if (ch.pre_s) {
@@ -98,7 +109,9 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
     else if (op.phase == PH_D) base = v2;
     else if (op.phase != PH_NONE) base = v3;  // FP and FF
     const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
-    for (int j0 = sub * ANG_JB; j0 < n_l; j0 += NSUB * ANG_JB) {
+    double2* ys_peer = ys;
+    if constexpr (CL == 2) ys_peer = cg::this_cluster().map_shared_rank(ys, crank ^ 1);
+    for (int j0 = gsub * ANG_JB; j0 < n_l; j0 += CL * NSUB * ANG_JB) {
       double2 acc[ANG_JB];
 #pragma unroll
       for (int q = 0; q < ANG_JB; ++q) acc[q] = make_double2(0.0, 0.0);
@@ -158,21 +171,24 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
             y = cmul_conj_phase(y, eta);
           }
           ys[j * RT + lr] = y;
+          if constexpr (CL == 2) ys_peer[j * RT + lr] = y;
         }
       }
     }
-    __syncthreads();
+    if constexpr (CL == 2) cg::this_cluster().sync();
+    else __syncthreads();
     double2* t = xs; xs = ys; ys = t;
   }
 
+  // both CTAs of a pair hold the whole result: each writes and reduces its share of l
   if (rv && xout)
-    for (int l = sub; l < n_l; l += NSUB) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * RT + lr];
+    for (int l = gsub; l < n_l; l += CL * NSUB) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * RT + lr];
 
   if (do_obs) {
     const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile<double2, RT>(g, xs, col, m, tile * RT, lr, sub, NSUB, rr, fr2);
+    observables_tile<double2, RT>(g, xs, col, m, tile * RT, lr, gsub, CL * NSUB, rr, fr2);
     const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
-    for (int L = sub; L < n_den; L += NSUB) {
+    for (int L = gsub; L < n_den; L += CL * NSUB) {
       const double d = density_multipole<double2, RT>(L, m, n_l, xs, lr, g.coef, g.n_m);
       if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
     }
@@ -181,16 +197,37 @@ k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* 
 
 size_t angular_smem_fp64(int n_l) { return 2 * (size_t)n_l * TR * sizeof(double2); }
 
+static int g_angular_sms = 148;
+
+template <int RT>
+static void launch_angular_rt(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
+                              cudaStream_t s) {
+  const int tiles = g.n_cols * ((g.n_r + RT - 1) / RT);
+  const size_t smem = 2 * (size_t)g.n_l * RT * sizeof(double2);
+  if (tiles >= 2 * g_angular_sms) {
+    k_angular_fp64<RT, 1><<<tiles, ANG_WARPS * 32, smem, s>>>(g, half, xin, xout, do_obs);
+    return;
+  }
+  // too few tiles to fill the GPU: a CTA pair per tile
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * tiles);
+  cfg.blockDim = dim3(ANG_WARPS * 32);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_angular_fp64<RT, 2>, g, half, xin, xout, do_obs);
+}
+
 void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
                          cudaStream_t s) {
-  const dim3 block(ANG_WARPS * 32);
-  if (g.obs_seg == 16) {
-    const dim3 grid(g.n_cols * ((g.n_r + 15) / 16));
-    k_angular_fp64<16><<<grid, block, 2 * (size_t)g.n_l * 16 * sizeof(double2), s>>>(g, half, xin, xout, do_obs);
-  } else {
-    const dim3 grid(g.n_cols * ((g.n_r + TR - 1) / TR));
-    k_angular_fp64<TR><<<grid, block, angular_smem_fp64(g.n_l), s>>>(g, half, xin, xout, do_obs);
-  }
+  if (g.obs_seg == 16) launch_angular_rt<16>(g, half, xin, xout, do_obs, s);
+  else launch_angular_rt<TR>(g, half, xin, xout, do_obs, s);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -628,9 +665,15 @@ cudaError_t configure_kernels_fp64(int n_l_max, int n_r_max) {
   if (e != cudaSuccess) return e;
   if (angular_smem_fp64(n_l_max) > (size_t)optin || 3 * (size_t)n_r_max * sizeof(double) > (size_t)optin)
     return cudaErrorInvalidValue;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR>, optin);
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR, 1>, optin);
   if (e != cudaSuccess) return e;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<16>, optin);
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<16, 1>, optin);
+  if (e != cudaSuccess) return e;
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR, 2>, optin);
+  if (e != cudaSuccess) return e;
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<16, 2>, optin);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&g_angular_sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   e = configure_radial_fp64();
   if (e != cudaSuccess) return e;
