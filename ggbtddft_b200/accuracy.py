@@ -279,7 +279,8 @@ def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed:
 
 
 def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64, seed: int = 0,
-                                angular: str = "theta", xc_frozen: bool = True, per_rung: int = 1) -> dict:
+                                angular: str = "theta", xc_frozen: bool = True, per_rung: int = 1,
+                                frozen: bool = False) -> dict:
     """Whole pulses of the argon focal scan: all runs batched in ``precision`` (one context, grid groups
     on concurrent streams, each run followed by zero field up to the longest pulse) against the FP64
     form of ``per_rung`` runs per grid rung, each stepped alone over its own pulse.  Per checked
@@ -287,7 +288,7 @@ def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64,
     summed over every l), the dipole L2 difference and the norm difference."""
     dr = P.argon_draws(n_runs, seed)
     runs = P.argon_ensemble(n_runs, seed=seed, device="cuda", xc_frozen=xc_frozen)
-    runs = [dataclasses.replace(r, angular=angular) for r in runs]
+    runs = [dataclasses.replace(r, angular=angular, use_hartree=0 if frozen else r.use_hartree) for r in runs]
     n = max(r.n_t for r in runs)
     tst, t_tst, st_tst = _batched_totals(runs, precision, n)
     checked = [i for members in dr.grid_groups().values() for i in members[:per_rung]]
@@ -307,8 +308,9 @@ def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64,
                         harmonic_rel_err_max=float(herr.max()), harmonic_rel_err=herr.tolist(),
                         dipole_rel_l2=float(np.linalg.norm(d_t - d_r) / np.linalg.norm(d_r)),
                         norm_drift_max=float(np.abs(tst[i]["norm"][:, :m] - ref[0]["norm"][:, :m]).max())))
-    return dict(config=f"argon focal scan, {n_runs} runs (seed {seed}), whole pulses, angular {angular}, "
-                       f"xc {'frozen at the ground state' if xc_frozen else 'adiabatic'}",
+    pot = "all potentials frozen at the ground state" if frozen else (
+        "xc frozen at the ground state" if xc_frozen else "adiabatic")
+    return dict(config=f"argon focal scan, {n_runs} runs (seed {seed}), whole pulses, angular {angular}, {pot}",
                 precision=precision, steps_stepped=n, seconds=dict(batched=t_tst, fp64_checked=t_ref),
                 batched_status=st_tst, per_instance=per,
                 harmonic_rel_err_max=max(q["harmonic_rel_err_max"] for q in per),
@@ -343,12 +345,14 @@ def main(argv=None):
                     help="instead: whole pulses of the 64-run argon ensemble, batched, against FP64 runs of "
                          "one run per grid rung")
     ap.add_argument("--xc-frozen", action="store_true", help="exchange-correlation held at the ground state")
+    ap.add_argument("--per-rung", type=int, default=1, help="--argon-ensemble-full: FP64 runs checked per rung")
     ap.add_argument("--sweep", action="store_true",
                     help="instead: FP64 self-sensitivity of argon LDA for dt in {0.02, 0.01, 0.005} and N_har "
                          "in {2, 3, 4} over the whole pulse")
     args = ap.parse_args(argv)
     if args.argon_ensemble_full:
-        rep = compare_argon_ensemble_full(args.precision, angular=args.angular, xc_frozen=args.xc_frozen)
+        rep = compare_argon_ensemble_full(args.precision, angular=args.angular, xc_frozen=args.xc_frozen,
+                                          frozen=args.frozen, per_rung=args.per_rung)
         if args.out:
             with open(args.out, "w") as f:
                 f.write(json.dumps(rep) + "\n")

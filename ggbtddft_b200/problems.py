@@ -176,7 +176,7 @@ def reference_like(n_r: int = 64, n_l: int = 32, n_t: int = 64, atom: str = "H",
 # Angular step of the benchmark configurations: "theta" (one phase per half-step at the Gauss nodes,
 # the form these configurations are benchmarked in) or "reference" (the reference's FF/FP/D/P/S chain,
 # the parity form).  The reference_like() runs always use the reference's chain.
-BENCH_ANGULAR = "reference"
+BENCH_ANGULAR = "theta"
 
 
 @dataclasses.dataclass

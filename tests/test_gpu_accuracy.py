@@ -3,9 +3,10 @@ semiclassical cutoff within 1e-3 (relative) of the FP64 form on the same inputs,
 and the dipole L2 difference it comes with.  HHG spectra are computed with the reference's recipe
 (spectrum.py, pinned to analysis.py).
 
-Hydrogen (N_r 200, l_max 32, 8,826 steps) and helium LDA with PW92 correlation (N_r 400, l_max 64,
-29,419 steps) are the well-conditioned configurations: two FP64 runs from initial orbitals 1e-10
-apart stay 1e-8 apart in the dipole over these pulses.
+Hydrogen (N_r 200, l_max 32, 8,826 steps) and helium LDA with PW92 correlation and every Hartree
+multipole L = 0 .. 2 l_max = 128 (N_r 400, l_max 64, 29,419 steps), both in the theta form the
+benchmark configurations use, are well-conditioned: two FP64 runs from initial orbitals 1e-10 apart
+stay 1e-8 apart in the dipole over these pulses.
 """
 import pytest
 

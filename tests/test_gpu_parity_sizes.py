@@ -52,13 +52,13 @@ def _centre(run, n):
 
 def test_fp64_helium_configuration_at_the_pulse_centre():
     """He LDA, N_r 400, r_max 200, l_max 64, PW92 correlation, cos^(1/8) mask: 16 steps."""
-    run = _centre(P.config_helium(device="cuda"), 16)
+    run = _centre(P.config_helium(device="cuda", angular="reference"), 16)
     _fp64_vs_oracle(run, 16)
 
 
 def test_fp64_argon_configuration_at_the_pulse_centre():
     """Ar LDA, N_r 600, r_max 300, l_max 96, nine orbitals, all couplings active: 12 steps."""
-    run = _centre(P.config_argon(device="cuda"), 12)
+    run = _centre(P.config_argon(device="cuda", angular="reference"), 12)
     _fp64_vs_oracle(run, 12)
 
 
