@@ -261,6 +261,17 @@ def measured_traffic(runs, groups, precision, phase):
     return total
 
 
+def chain_products(run) -> int:
+    """Products of one angular half-step: the theta form's two (to the P coupling's eigenbasis and
+    back); the reference chain's active couplings + 1 (adjacent rotations pre-multiplied): FF with
+    N_har >= 4, FP and D with N_har >= 3 when Hartree is on, always P."""
+    if getattr(run, "angular", "reference") == "theta":
+        return 2
+    h = run.use_hartree == 1 and run.target_id > 0
+    k = 1 + (2 if h and run.n_har >= 3 else 0) + (1 if h and run.n_har >= 4 else 0)
+    return k + 1
+
+
 def phase_traffic(runs, groups, precision):
     """Algorithmic bytes and flops of each phase of one step, summed over the grid groups.
 
@@ -280,7 +291,7 @@ def phase_traffic(runs, groups, precision):
         n_r, n_l = r0.n_r, r0.n_l
         cols = sum(runs[i].n_orb for i in members)
         elems = n_r * n_l * cols
-        n_gemm = 2 + (3 if (r0.use_hartree and r0.target_id > 0 and r0.n_har >= 4) else 0)
+        n_gemm = chain_products(r0)
         out["radial"]["bytes"] += wb * n_r * n_r * n_l + (xin + cb) * elems
         out["radial"]["flops"] += 8.0 * n_r * n_r * n_l * cols
         for k in ("angular_first", "angular_second"):

@@ -6,8 +6,16 @@ import pytest
 import bench
 
 
-def _run(n_r, l_max, n_orb=9, hartree=True):
-    return SimpleNamespace(n_r=n_r, n_l=l_max + 1, n_orb=n_orb, use_hartree=hartree, target_id=1, n_har=4)
+def _run(n_r, l_max, n_orb=9, hartree=True, angular="reference", n_har=4):
+    return SimpleNamespace(n_r=n_r, n_l=l_max + 1, n_orb=n_orb, use_hartree=hartree, target_id=1, n_har=n_har,
+                           angular=angular)
+
+
+def test_chain_products_per_half_step():
+    assert bench.chain_products(_run(600, 96)) == 5                     # FF, FP, D, P + 1
+    assert bench.chain_products(_run(600, 96, n_har=3)) == 4            # FP, D, P + 1
+    assert bench.chain_products(_run(600, 96, hartree=False)) == 2      # P + 1
+    assert bench.chain_products(_run(600, 96, angular="theta")) == 2   # one phase at the nodes
 
 
 def test_phase_bytes_and_flops_of_one_int8_group():
