@@ -275,11 +275,13 @@ class GridRung:
 
 
 # Grid ladders.  Runs are binned onto a few grids so that the runs of one grid share W (the radial
-# propagators depend on the atom, the grid, dt and the absorber, not on the laser).
-ARGON_LADDER = [GridRung(600, 300.0, 96), GridRung(700, 350.0, 112), GridRung(800, 400.0, 128),
+# propagators depend on the atom, the grid, dt and the absorber, not on the laser).  l_max 127 rather
+# than 128: N_l = 128 channels fill one 128-row tensor-core tile of the int8 angular chain, where 129
+# would need a second, nearly empty one (half the radii per CTA).
+ARGON_LADDER = [GridRung(600, 300.0, 96), GridRung(700, 350.0, 112), GridRung(800, 400.0, 127),
                 GridRung(900, 450.0, 144), GridRung(1000, 500.0, 160)]
 HHE_LADDER = [GridRung(200, 100.0, 32), GridRung(400, 200.0, 64), GridRung(600, 300.0, 96),
-              GridRung(800, 400.0, 128)]
+              GridRung(800, 400.0, 127)]
 
 
 def quiver_radius(laser: LaserSpec) -> float:
