@@ -328,7 +328,8 @@ def run_ours(args, rank, world, dist):
     runs, precision, desc = workload_runs(args.workload, n_t, device="cuda", split=args.precision,
                                           angular=args.angular, potentials=args.potentials)
     units_per_step = sum(r.n_orb for r in runs)
-    tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t)
+    tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t,
+                         autotune=bool(args.autotune) and precision == "split_int8")
     stream = torch.cuda.Stream()
     h = stream.cuda_stream
     hbm_peak, _, peak_kind = read_peaks()
@@ -372,7 +373,7 @@ def run_ours(args, rank, world, dist):
     # end to end through the C ABI from host buffers
     if not args.e2e:
         e2e_value, h2d, d2h = None, 0, 0
-    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t) if args.e2e else None
+    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t, tuning=tp.tuning) if args.e2e else None
     if tp2 is not None:
         tp2.step(args.warmup)
         torch.cuda.synchronize()
@@ -558,6 +559,9 @@ def main():
                          "reference's coupling chain")
     ap.add_argument("--potentials", default=DEFAULT_POTENTIALS, choices=sorted(POTENTIALS),
                     help="how the runs' potentials evolve: " + "; ".join(f"{k}: {v}" for k, v in POTENTIALS.items()))
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="1: radial tiles of the int8 form from the autotuner (shipped B200 tunings; times the "
+                         "candidates of a group shape it has not seen)")
     ap.add_argument("--clocks-csv", default=None,
                     help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")

@@ -7,7 +7,7 @@ most stages that fit.  The tuner times every candidate on the group's own runs (
 launched alone, CUDA events, after warm-up) and keeps the fastest.  Results are cached in a JSON
 file keyed on the GPU's name, the library version and the group's (N_r, l_max, orbital columns), so
 a grid shape is timed once per GPU model and kernel version; the cache is $GGB_AUTOTUNE_CACHE, else
-~/.cache/ggbtddft_b200/autotune.json.
+~/.cache/ggbtddft_b200/autotune.json, read over the tunings shipped in tuning/autotune_b200.json.
 
     TimePropagation(runs, precision="split_int8", autotune=True)   # cached or tuned tiles
     tuning_for(runs, groups)                                         # {group: (bn, stages)}
@@ -63,7 +63,12 @@ def candidates(n_cols: int) -> List[Tuple[int, int]]:
     return out
 
 
+# tunings measured on B200 for the benchmark ensembles' grid groups, shipped with the package
+PACKAGED_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "autotune_b200.json")
+
+
 def cache_path() -> str:
+    """$GGB_AUTOTUNE_CACHE, else the user cache ~/.cache/ggbtddft_b200/autotune.json."""
     return os.environ.get("GGB_AUTOTUNE_CACHE") or os.path.join(
         os.path.expanduser("~"), ".cache", "ggbtddft_b200", "autotune.json")
 
@@ -136,7 +141,8 @@ def tuning_for(runs: Sequence, groups: Sequence[Sequence[int]], cache_file: Opti
                timer: Callable = time_candidate, device_name: Optional[str] = None) -> Dict[int, Tuple[int, int]]:
     """{group index: (bn, stages)} from the cache, timing the groups that miss it."""
     path = cache_file or cache_path()
-    cache = load_cache(path)
+    cache = load_cache(PACKAGED_CACHE)
+    cache.update(load_cache(path))
     if device_name is None:
         import torch
         device_name = torch.cuda.get_device_name()
@@ -152,3 +158,24 @@ def tuning_for(runs: Sequence, groups: Sequence[Sequence[int]], cache_file: Opti
     if dirty:
         save_cache(path, cache)
     return out
+
+
+def main(argv=None):
+    """Tune the grid groups of the benchmark ensembles on this GPU and write them to the packaged cache:
+    python -m ggbtddft_b200.autotune [--out PATH]"""
+    import argparse
+    import dataclasses
+    from . import problems as P
+    from .engine import group_runs
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=PACKAGED_CACHE)
+    args = ap.parse_args(argv)
+    for runs in (P.argon_ensemble(64, seed=0, n_steps=16, device="cuda"),
+                 P.hhe_ensemble(256, seed=0, n_steps=16, device="cuda")):
+        runs = [dataclasses.replace(r, angular="theta") for r in runs]
+        groups = group_runs(runs)
+        print(json.dumps({str(k): v for k, v in tuning_for(runs, groups, cache_file=args.out).items()}))
+
+
+if __name__ == "__main__":
+    main()

@@ -503,7 +503,7 @@ static int launch_init(ggb_ctx* ctx, GroupHost& g, cudaStream_t s) {
 // ----------------------------------------------------------------------------------------------
 extern "C" {
 
-const char* ggb_version(void) { return "ggbtddft-b200 0.1 (sm_100a)"; }
+const char* ggb_version(void) { return "ggbtddft-b200 0.2 (sm_100a)"; }
 
 int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run_desc* runs, ggb_ctx** out) {
   if (!out) return GGB_ERR_ARG;
