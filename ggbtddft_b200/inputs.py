@@ -546,7 +546,11 @@ def ground_state(grid: RadialGrid, Z: float, orbitals: Sequence[Orbital], intera
     out of this path's scope; this self-consistent loop provides the same kind of input:
     occupied radial orbitals u and the static potential vscf that enters W_l.
     For ``interacting=False`` it diagonalises -T/2 - Z/r once (hydrogen-like).
+    With ``device`` (a torch device name) the whole loop runs there (``ground_state_device``).
     """
+    if device is not None:
+        return ground_state_device(grid, Z, orbitals, interacting, correlation=correlation,
+                                   iterations=iterations, mix=mix, tol=tol, device=device)
     v_ion = -Z / grid.r
     ls = sorted({o.l for o in orbitals})
     vscf = np.zeros(grid.n_r)
@@ -578,6 +582,77 @@ def ground_state(grid: RadialGrid, Z: float, orbitals: Sequence[Orbital], intera
             if dv < tol:
                 break
     return GroundState(list(orbitals), u, en, v_ion, vscf, np.zeros(grid.n_r))
+
+
+def ground_state_device(grid: RadialGrid, Z: float, orbitals: Sequence[Orbital], interacting: bool,
+                        correlation: bool = False, iterations: int = 200, mix: float = 0.3,
+                        tol: float = 1e-11, device: str = "cuda") -> GroundState:
+    """``ground_state`` with every array resident on ``device`` (torch, FP64).
+
+    Per iteration: one batched symmetric eigensolve of the radial Hamiltonians of all occupied l,
+    the orbital density, the Hartree monopole v(r_a) = sum_b rho0(b)/max(r_a, r_b), Slater exchange
+    and PW92 correlation, linear mixing; one scalar (max |v_new - vscf|, the convergence test) is
+    read back per iteration.  Same iteration, mixing and stopping rule as the host loop, so the two
+    reach the same fixed point (to the eigensolvers' rounding).
+    """
+    import torch
+    dev = torch.device(device)
+    f64 = torch.float64
+    r = torch.from_numpy(grid.r).to(dev, f64)
+    T = torch.from_numpy(grid.T).to(dev, f64)
+    ls = sorted({o.l for o in orbitals})
+    lt = torch.tensor(ls, dtype=f64, device=dev)
+    cent = lt[:, None] * (lt[:, None] + 1.0) / 2.0 / r[None, :] ** 2          # [n_ls, N_r]
+    li = torch.tensor([ls.index(o.l) for o in orbitals], device=dev)
+    ki = torch.tensor([o.n - o.l - 1 for o in orbitals], device=dev)
+    rows = torch.arange(len(orbitals), device=dev)
+    v_ion = -Z / r
+    n_g = grid.n_g
+    drdx = torch.from_numpy(grid.drdx).to(dev, f64)
+    p2 = torch.from_numpy(np.power(grid.P, 2.0)).to(dev, f64)
+    r2 = r ** 2
+    inv_rmax = 1.0 / torch.maximum(r[:, None], r[None, :])
+
+    def solve(vtot):
+        H = -0.5 * T[None] + torch.diag_embed(vtot[None, :] + cent)
+        H = 0.5 * (H + H.transpose(1, 2))
+        e, U = torch.linalg.eigh(H)
+        u = U[li, :, ki]                                       # [n_orb, N_r]
+        big = u[rows, u.abs().argmax(dim=1)]
+        u = torch.where((big < 0)[:, None], -u, u)
+        return u, e[li, ki]
+
+    def xc(n):
+        v = -torch.pow(3.0 / math.pi * torch.clamp(n, min=0.0), 1.0 / 3.0)
+        if correlation:
+            a, a1, b1, b2, b3, b4 = 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294
+            nc = torch.clamp(n, min=1e-300)
+            rs = torch.pow(3.0 / (4.0 * math.pi * nc), 1.0 / 3.0)
+            srs = torch.sqrt(rs)
+            q0 = -2.0 * a * (1.0 + a1 * rs)
+            q1 = 2.0 * a * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs)
+            q1p = a * (b1 / srs + 2.0 * b2 + 3.0 * b3 * srs + 4.0 * b4 * rs)
+            lg = torch.log1p(1.0 / q1)
+            ec = q0 * lg
+            dec = -2.0 * a * a1 * lg - q0 * q1p / (q1 * q1 + q1)
+            v = v + (ec - rs / 3.0 * dec)
+        return v
+
+    u, en = solve(v_ion)
+    vscf = torch.zeros_like(r)
+    if interacting:
+        occ = torch.tensor([float(o.occ) for o in orbitals], dtype=f64, device=dev)
+        for _ in range(iterations):
+            rho0 = (occ[:, None] * u ** 2).sum(dim=0)
+            n = n_g * (n_g + 1) / 2.0 * (rho0 / (4.0 * math.pi)) / drdx * p2 / r2
+            v_new = (rho0[None, :] * inv_rmax).sum(dim=1) + xc(n)
+            dv = (v_new - vscf).abs().max()
+            vscf = (1.0 - mix) * vscf + mix * v_new
+            u, en = solve(v_ion + vscf)
+            if float(dv) < tol:
+                break
+    return GroundState(list(orbitals), u.cpu().numpy(), en.cpu().numpy(), -Z / grid.r,
+                       vscf.cpu().numpy(), np.zeros(grid.n_r))
 
 
 # Orbital sets of the benchmark atoms.  m = -1 is stored as m = 1: the length-gauge couplings of a

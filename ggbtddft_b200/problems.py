@@ -16,11 +16,21 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import time
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
 from . import inputs as I
+
+# Wall-clock seconds spent in the one-time input producers (ground-state SCF, radial propagators,
+# angular eigensystems) since the last ``reset_setup_seconds()``: set-up, reported beside the step rate.
+SETUP_SECONDS: Dict[str, float] = {"ground_state": 0.0, "radial_propagators": 0.0, "angular": 0.0}
+
+
+def reset_setup_seconds() -> None:
+    for k in SETUP_SECONDS:
+        SETUP_SECONDS[k] = 0.0
 
 
 @dataclasses.dataclass
@@ -106,9 +116,13 @@ def build_run(grid: I.RadialGrid, n_l: int, dt: float, gs: I.GroundState, E: np.
     else:
         raise ValueError(absorber)
     if W is None:
+        t0 = time.perf_counter()
         W = I.radial_propagators(grid, n_l, dt, v0, gs.vscf, mask_r, row_mask=row_mask, device=device)
+        SETUP_SECONDS["radial_propagators"] += time.perf_counter() - t0
     n_m = int(max(o.m for o in gs.orbitals)) + 1
+    t0 = time.perf_counter()
     ang = I.angular_eigensystems(n_l, n_m)
+    SETUP_SECONDS["angular"] += time.perf_counter() - t0
     return RunInputs(
         grid=grid, n_l=n_l, dt=dt, W=W,
         V={c: ang[c][0] for c in I.COUPLINGS}, D={c: ang[c][1] for c in I.COUPLINGS},
@@ -226,8 +240,10 @@ def baseline_run(atom: str, n_r: int, r_max: float, l_max: int, dt: float, laser
     key = (atom, n_r, r_max)
     gs = None if gs_cache is None else gs_cache.get(key)
     if gs is None:
+        t0 = time.perf_counter()
         gs = I.ground_state(grid, spec.Z, spec.orbitals, interacting=spec.interacting,
                             correlation=spec.correlation, device=device)
+        SETUP_SECONDS["ground_state"] += time.perf_counter() - t0
         if gs_cache is not None:
             gs_cache[key] = gs
     full = I.steps_for_sin2(dt, laser.omega, laser.cycles)

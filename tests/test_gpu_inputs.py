@@ -30,3 +30,20 @@ def test_angular_eigensystems_built_on_the_gpu_equal_the_cpu_build(n_l, n_m):
                 U = V[m] @ np.diag(np.exp(-1j * a * D[m])) @ V[m].T
                 Ug = Vg[m] @ np.diag(np.exp(-1j * a * Dg[m])) @ Vg[m].T
                 assert np.abs((U - Ug)[m:, m:]).max() < 1e-12, (c, m)
+
+
+def test_ground_state_scf_on_the_gpu_equals_the_host_loop():
+    """Argon LDA + PW92 on the 600-point grid of the benchmark: the device-resident loop (batched
+    eigensolves, density, Hartree monopole and exchange-correlation on the GPU) reaches the host
+    loop's fixed point."""
+    import time
+    g = I.make_grid(600, 300.0, I.zeta_physical_to_ref(0.5, 300.0))
+    t0 = time.perf_counter()
+    a = I.ground_state(g, 18.0, I.ORBITALS_AR, True, correlation=True)
+    t1 = time.perf_counter()
+    b = I.ground_state(g, 18.0, I.ORBITALS_AR, True, correlation=True, device="cuda")
+    t2 = time.perf_counter()
+    print(f"argon N_r 600 SCF: host {t1 - t0:.2f} s, GPU {t2 - t1:.2f} s")
+    assert np.abs(a.vscf - b.vscf).max() < 1e-9
+    assert np.abs(a.energies - b.energies).max() < 1e-9 * np.abs(a.energies).max()
+    assert np.abs(a.u - b.u).max() < 1e-9
