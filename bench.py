@@ -182,11 +182,14 @@ def compute_peaks(stream_handle):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """nvidia-smi clocks/throttle sampling during the timed region: the sampler is started and its
+    first sample awaited before the region opens; only the samples written after that count."""
 
-    def __init__(self, index: int, path: str = None):
+    def __init__(self, index: int, path: str = None, period_ms: int = 50):
         self.index = index
         self.proc = None
+        self.period_ms = period_ms
+        self.skip = 0
         self.path = path or os.path.join(tempfile.mkdtemp(prefix="ggb_clocks_"), f"clocks_gpu{index}.csv")
 
     def __enter__(self):
@@ -198,7 +201,16 @@ class ClockSampler:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 10.0 and self.proc.poll() is None:
+                with open(self.path) as fh:
+                    n = sum(1 for line in fh if line.endswith("\n"))
+                if n > 0:
+                    self.skip = n
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -217,7 +229,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = open(self.path).readlines()
+        # the samples of the timed region; if it was shorter than one period, the one just before it
+        lines = lines[self.skip:] if len(lines) > self.skip else lines[-1:]
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -298,6 +313,12 @@ def phase_traffic(runs, groups, precision):
             out[k]["bytes"] += 2 * cb * elems
             out[k]["flops"] += n_gemm * 4.0 * n_l * n_l * n_r * cols
     return out
+
+
+def phase_bound_seconds(tf, hbm_gbs: float, arith_tera: float) -> float:
+    """Roofline time of one step whose phases run one after another: sum over phases of
+    max(algorithmic bytes / HBM peak, algorithmic flops / arithmetic peak)."""
+    return sum(max(v["bytes"] / (hbm_gbs * 1e9), v["flops"] / (arith_tera * 1e12)) for v in tf.values())
 
 
 # ---------------------------------------------------------------------------------------------
@@ -446,14 +467,17 @@ def run_ours(args, rank, world, dist):
                         peak_kind="measured (ggb_measure_peaks)")
     if precision != "fp64":
         roofline["tensor_frac_executed"] = d["tensor_frac_executed"]
-    # the whole step against its own bound: algorithmic bytes and flops of all phases
+    # the whole step against its own bound: the phases run one after another, so the bound is the
+    # sum over phases of each phase's own bound (algorithmic bytes at the HBM peak or flops at the
+    # arithmetic peak, whichever takes longer)
     step_bytes = sum(tf[k]["bytes"] for k in tf)
     step_flops = sum(tf[k]["flops"] for k in tf)
     step_s = ms_max / args.steps / 1e3 / world
+    step_bound = phase_bound_seconds(tf, hbm_peak, arith_peak)
     roofline["step"] = dict(ms=round(ms_max / args.steps, 4), algorithmic_bytes=int(step_bytes),
-                            algorithmic_flops=int(step_flops),
-                            bound_ms=round(1e3 * max(step_bytes / (hbm_peak * 1e9), step_flops / (arith_peak * 1e12)), 4),
-                            frac=round(max(step_bytes / (hbm_peak * 1e9), step_flops / (arith_peak * 1e12)) / step_s, 4))
+                            algorithmic_flops=int(step_flops), bound_ms=round(1e3 * step_bound, 4),
+                            frac=round(step_bound / step_s, 4),
+                            bound_how="sum over phases of max(bytes / HBM peak, flops / arithmetic peak)")
     # the same runs stepped one at a time in the plain FP64 form (per-instance launches), on this GPU,
     # with that form's own roofline (its step's algorithmic bytes and flops against the HBM and the
     # measured FP64 peak)
@@ -473,9 +497,7 @@ def run_ours(args, rank, world, dist):
             per_step = a.elapsed_time(b) / 1e3 / k
             one.close()
             t1 = phase_traffic([runs[members[0]]], [[0]], "fp64")
-            by = sum(t1[q]["bytes"] for q in t1)
-            fl = sum(t1[q]["flops"] for q in t1)
-            bound_s += len(members) * max(by / (hbm_peak * 1e9), fl / (peaks["fp64_tflops"] * 1e12))
+            bound_s += len(members) * phase_bound_seconds(t1, hbm_peak, peaks["fp64_tflops"])
             total_s += per_step * len(members)
             units += sum(runs[i].n_orb for i in members)
         rate = units / total_s
@@ -483,8 +505,9 @@ def run_ours(args, rank, world, dist):
                          how="each run of the workload stepped alone in the FP64 form (one time per grid, "
                              "weighted by the runs on it), same GPU", speedup=round(value / rate, 2),
                          roofline_frac=round(bound_s / total_s, 4),
-                         roofline_how="per run-step: max(algorithmic bytes / HBM peak, algorithmic flops / "
-                                      "measured FP64 peak) over the measured time, weighted like the rate")
+                         roofline_how="per run-step: sum over its phases of max(algorithmic bytes / HBM peak, "
+                                      "algorithmic flops / measured FP64 peak), over the measured time, weighted "
+                                      "like the rate")
     return dict(value=value, ms=ms_max, units_per_step=units_per_step, desc=desc, precision=precision,
                 clocks=clk.summary(), roofline=roofline,
                 e2e=None if e2e_value is None else dict(

@@ -55,3 +55,12 @@ def test_cpu_sample_covers_every_grid_group_once(name, total):
         for idx, count, _ in groups:
             same = [i for i in range(64) if dr.rung[i] == dr.rung[idx]]
             assert len(same) == count and idx == same[0]
+
+
+def test_step_bound_is_the_sum_of_phase_bounds():
+    """Phases run one after another: an HBM-bound radial product and a flop-bound angular chain do
+    not overlap, so the step's roofline time adds their bounds."""
+    tf = {"radial": dict(bytes=6.45e12, flops=1e12), "angular_first": dict(bytes=1e6, flops=36.6e12),
+          "angular_second": dict(bytes=6.45e11, flops=0.0)}
+    s = bench.phase_bound_seconds(tf, 6450.0, 36.6)
+    assert abs(s - (1.0 + 1.0 + 0.1)) < 1e-12
