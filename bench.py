@@ -140,6 +140,7 @@ DEFAULT_WORKLOAD = "ar-ens64"
 # arithmetic; the frozen-potential ensemble can, and is checked instance by instance
 DEFAULT_ANGULAR = "theta"
 DEFAULT_POTENTIALS = "frozen"
+DEFAULT_ANGULAR_ARITH = "int8"
 # tensor-core products executed per algorithmic real product, and the peak they run against
 SPLIT_PRODUCTS = {"split_bf16": 5,    # W_h x_h + W_h x_l + W_m x_h + W_m x_l + W_l x_h (BF16)
                   "split_int8": 10}   # int8 slice pairs (j, m), 0-based, with j + m <= 3
@@ -359,7 +360,11 @@ def run_ours(args, rank, world, dist):
                      "closed form), the rest is the laser fields and initial orbitals")
     units_per_step = sum(r.n_orb for r in runs)
     tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t,
-                         autotune=bool(args.autotune) and precision == "split_int8")
+                         autotune=bool(args.autotune) and precision == "split_int8",
+                         angular_fp64=args.angular_arith == "fp64")
+    if precision == "split_int8":
+        desc = dict(desc, angular_products="FP64 tensor cores (mma.sync m8n8k4 f64)" if tp.angular_fp64 else
+                    "int8 slice products on tcgen05 (31-bit operands, exact int32 accumulation)")
     stream = torch.cuda.Stream()
     h = stream.cuda_stream
     hbm_peak, _, peak_kind = read_peaks()
@@ -403,7 +408,8 @@ def run_ours(args, rank, world, dist):
     # end to end through the C ABI from host buffers
     if not args.e2e:
         e2e_value, h2d, d2h = None, 0, 0
-    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t, tuning=tp.tuning) if args.e2e else None
+    tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t, tuning=tp.tuning,
+                          angular_fp64=tp.angular_fp64) if args.e2e else None
     if tp2 is not None:
         tp2.step(args.warmup)
         torch.cuda.synchronize()
@@ -434,6 +440,13 @@ def run_ours(args, rank, world, dist):
     arith_unit = {"fp64": "TFLOP/s (FP64 FMA)", "split_int8": "TOP/s (tcgen05 kind::i8)",
                   "split_bf16": "TFLOP/s (bf16, cuBLAS-measured)"}[precision]
     sp = SPLIT_PRODUCTS.get(precision, 1)
+    # each phase's arithmetic against the peak of the unit it runs on (the int8 form with FP64
+    # angular products: the angular phases against the FP64 peak)
+    phase_peak = {k: arith_peak for k in ("radial", "angular_first", "angular_second")}
+    phase_split = {k: sp for k in phase_peak}
+    if tp.angular_fp64:
+        for k in ("angular_first", "angular_second"):
+            phase_peak[k], phase_split[k] = peaks["fp64_tflops"], 1
     kernels = {}
     for k in ("radial", "angular_first", "angular_second"):
         sec = phase_ms[k] / 1e3
@@ -441,14 +454,15 @@ def run_ours(args, rank, world, dist):
                           algorithmic_flops=int(tf[k]["flops"]),
                           gbs=round(tf[k]["bytes"] / sec / 1e9, 1), tflops=round(tf[k]["flops"] / sec / 1e12, 3),
                           hbm_frac=round(tf[k]["bytes"] / sec / 1e9 / hbm_peak, 4),
-                          arith_frac=round(tf[k]["flops"] / sec / 1e12 / arith_peak, 4))
-        if precision != "fp64":
-            kernels[k]["tensor_frac_executed"] = round(sp * tf[k]["flops"] / sec / 1e12 / arith_peak, 4)
+                          arith_frac=round(tf[k]["flops"] / sec / 1e12 / phase_peak[k], 4))
+        if precision != "fp64" and phase_split[k] > 1:
+            kernels[k]["tensor_frac_executed"] = round(phase_split[k] * tf[k]["flops"] / sec / 1e12 / phase_peak[k], 4)
     kernels["finalize"] = dict(ms=round(phase_ms["finalize"], 5))
     names = {"radial": {"fp64": "k_radial_fp64", "split_bf16": "k_radial_tc_persistent (tcgen05 kind::f16)",
                         "split_int8": "k_radial_i8 (tcgen05 kind::i8, int8 slices, int32 accumulation)"},
-             "angular": {"fp64": "k_angular_fp64", "split_bf16": "k_angular_tc (tcgen05 kind::f16)",
-                         "split_int8": "k_angular_i8 (tcgen05 kind::i8 chain, FP64 phases)"}}
+             "angular": {"fp64": "k_angular_fp64 (mma.sync f64)", "split_bf16": "k_angular_tc (tcgen05 kind::f16)",
+                         "split_int8": ("k_angular_fp64 (mma.sync f64)" if tp.angular_fp64 else
+                                        "k_angular_i8 (tcgen05 kind::i8 chain, FP64 phases)")}}
     d = kernels[dom]
     kname = names["radial" if dom == "radial" else "angular"][precision]
     est = measured_traffic(runs, tp.groups, precision, dom)
@@ -457,15 +471,20 @@ def run_ours(args, rank, world, dist):
                     traffic_source=None if est is None else TRAFFIC_SOURCE,
                     peak_kind=f"{peak_kind} hbm_gbs", dominant_by_time=dom,
                     peaks_measured=dict(hbm_gbs=hbm_peak, fp64_tflops=round(peaks["fp64_tflops"], 2),
+                                        fp64_fma_tflops=round(peaks["fp64_fma_tflops"], 2),
+                                        fp64_mma_tflops=round(peaks["fp64_mma_tflops"], 2),
                                         int8_tops=round(peaks["int8_tops"], 1),
-                                        how="FP64 FMA and tcgen05 kind::i8 microbenchmarks of this library "
-                                            "(ggb_measure_peaks); HBM: copy bandwidth of MEASURED_PEAKS.json"),
+                                        how="FP64 FMA, FP64 mma.sync and tcgen05 kind::i8 microbenchmarks of "
+                                            "this library (ggb_measure_peaks, ggb_measure_peak_fp64_mma; the FP64 "
+                                            "roofline takes the larger FP64 figure); HBM: copy bandwidth of "
+                                            "MEASURED_PEAKS.json"),
                     kernels=kernels)
     if d["arith_frac"] > d["hbm_frac"]:
+        fp64_unit = tp.angular_fp64 and dom != "radial"
         roofline.update(bound="tensor" if precision != "fp64" else "fp64", achieved=d["tflops"],
-                        peak=round(arith_peak, 2), unit=arith_unit, frac=d["arith_frac"],
-                        peak_kind="measured (ggb_measure_peaks)")
-    if precision != "fp64":
+                        peak=round(phase_peak[dom], 2), unit=arith_unit if not fp64_unit else "TFLOP/s (FP64)",
+                        frac=d["arith_frac"], peak_kind="measured (ggb_measure_peaks)")
+    if "tensor_frac_executed" in d:
         roofline["tensor_frac_executed"] = d["tensor_frac_executed"]
     # the whole step against its own bound: the phases run one after another, so the bound is the
     # sum over phases of each phase's own bound (algorithmic bytes at the HBM peak or flops at the
@@ -473,7 +492,7 @@ def run_ours(args, rank, world, dist):
     step_bytes = sum(tf[k]["bytes"] for k in tf)
     step_flops = sum(tf[k]["flops"] for k in tf)
     step_s = ms_max / args.steps / 1e3 / world
-    step_bound = phase_bound_seconds(tf, hbm_peak, arith_peak)
+    step_bound = sum(phase_bound_seconds({k: v}, hbm_peak, phase_peak.get(k, arith_peak)) for k, v in tf.items())
     roofline["step"] = dict(ms=round(ms_max / args.steps, 4), algorithmic_bytes=int(step_bytes),
                             algorithmic_flops=int(step_flops), bound_ms=round(1e3 * step_bound, 4),
                             frac=round(step_bound / step_s, 4),
@@ -594,6 +613,9 @@ def main():
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: radial tiles of the int8 form from the autotuner (shipped B200 tunings; times the "
                          "candidates of a group shape it has not seen)")
+    ap.add_argument("--angular-arith", default=DEFAULT_ANGULAR_ARITH, choices=["int8", "fp64"],
+                    help="split_int8 form: the angular products as int8 slice products on tcgen05 (int8) or on "
+                         "the FP64 tensor cores with mma.sync (fp64); the radial product stays int8")
     ap.add_argument("--clocks-csv", default=None,
                     help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")

@@ -35,8 +35,8 @@ from .engine import TimePropagation
 IONISATION_POTENTIAL = {"H": 0.5, "He": 0.9036, "Ar": 0.5792}   # Ha (experimental first Ip)
 
 
-def _run(run: P.RunInputs, precision: str, n_steps: int, chunk: int = 4096):
-    tp = TimePropagation([run], precision=precision, per_l=True, n_t=n_steps)
+def _run(run: P.RunInputs, precision: str, n_steps: int, chunk: int = 4096, angular_fp64: bool = False):
+    tp = TimePropagation([run], precision=precision, per_l=True, n_t=n_steps, angular_fp64=angular_fp64)
     t0 = time.perf_counter()
     done = 0
     while done < n_steps:
@@ -77,10 +77,11 @@ def _errors(run, ref, tst, atom, e0):
 
 
 def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_int8", n_steps: Optional[int] = None,
-                  e0: Optional[float] = None, sensitivity: float = 0.0) -> dict:
+                  e0: Optional[float] = None, sensitivity: float = 0.0, angular_fp64: bool = False) -> dict:
+    """``angular_fp64``: the split form with its angular products on the FP64 tensor cores."""
     n = run.n_t if n_steps is None else n_steps
     ref = _run(run, "fp64", n)
-    tst = _run(run, precision, n)
+    tst = _run(run, precision, n, angular_fp64=angular_fp64)
     e0 = float(np.abs(run.E).max()) if e0 is None else e0
     fp64_self = None
     if sensitivity > 0:
@@ -220,10 +221,10 @@ def sensitivity_sweep(variants=((0.02, 4), (0.01, 4), (0.005, 4), (0.02, 3), (0.
                 dipole_vs_dt002_rel_l2=conv)
 
 
-def _batched_totals(runs, precision: str, n_steps: int, chunk: int = 4096):
+def _batched_totals(runs, precision: str, n_steps: int, chunk: int = 4096, angular_fp64: bool = False):
     """All runs in one context (grid groups on concurrent streams); occupation-weighted total dipole
     (sum over every l) and norms of each run, and the seconds the stepping took."""
-    tp = TimePropagation(runs, precision=precision, per_l=False, n_t=n_steps)
+    tp = TimePropagation(runs, precision=precision, per_l=False, n_t=n_steps, angular_fp64=angular_fp64)
     t0 = time.perf_counter()
     done = 0
     while done < n_steps:
@@ -240,7 +241,7 @@ def _batched_totals(runs, precision: str, n_steps: int, chunk: int = 4096):
 
 
 def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed: int = 0,
-                         angular: str = "reference") -> dict:
+                         angular: str = "reference", angular_fp64: bool = False) -> dict:
     """The 256-run H/He focal scan over every run's whole pulse: the batched ``precision`` form against
     the batched FP64 form (the same runs, grid groups and field samples).  Each run's pulse is
     followed by zero field up to the longest pulse; each run's spectrum is taken over its own
@@ -253,7 +254,7 @@ def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed:
         runs = [dataclasses.replace(r, angular=angular) for r in runs]
     n = max(r.n_t for r in runs)
     ref, t_ref, st_ref = _batched_totals(runs, "fp64", n)
-    tst, t_tst, st_tst = _batched_totals(runs, precision, n)
+    tst, t_tst, st_tst = _batched_totals(runs, precision, n, angular_fp64=angular_fp64)
     per = []
     for i, r in enumerate(runs):
         m = r.n_t
@@ -270,7 +271,7 @@ def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed:
                         norm_drift_max=float(np.abs(tst[i]["norm"][:, :m] - ref[i]["norm"][:, :m]).max())))
     worst = max(per, key=lambda q: q["harmonic_rel_err_max"])
     return dict(config=f"H/He focal scan, {n_runs} runs (seed {seed}), whole pulses", precision=precision,
-                angular=angular, steps_stepped=n, seconds=dict(fp64=t_ref, split=t_tst),
+                angular=angular, angular_products="FP64 (mma.sync)" if angular_fp64 else "int8 slices", steps_stepped=n, seconds=dict(fp64=t_ref, split=t_tst),
                 status=dict(fp64=st_ref, split=st_tst), per_instance=per,
                 harmonic_rel_err_max=worst["harmonic_rel_err_max"], worst_instance=worst,
                 instances_within_1e3=int(sum(q["harmonic_rel_err_max"] <= 1e-3 for q in per)),
@@ -280,7 +281,7 @@ def compare_hhe_ensemble(precision: str = "split_int8", n_runs: int = 256, seed:
 
 def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64, seed: int = 0,
                                 angular: str = "theta", xc_frozen: bool = True, per_rung: int = 1,
-                                frozen: bool = False) -> dict:
+                                frozen: bool = False, angular_fp64: bool = False) -> dict:
     """Whole pulses of the argon focal scan: all runs batched in ``precision`` (one context, grid groups
     on concurrent streams, each run followed by zero field up to the longest pulse) against the FP64
     form of ``per_rung`` runs per grid rung, each stepped alone over its own pulse.  Per checked
@@ -290,7 +291,7 @@ def compare_argon_ensemble_full(precision: str = "split_int8", n_runs: int = 64,
     runs = P.argon_ensemble(n_runs, seed=seed, device="cuda", xc_frozen=xc_frozen)
     runs = [dataclasses.replace(r, angular=angular, use_hartree=0 if frozen else r.use_hartree) for r in runs]
     n = max(r.n_t for r in runs)
-    tst, t_tst, st_tst = _batched_totals(runs, precision, n)
+    tst, t_tst, st_tst = _batched_totals(runs, precision, n, angular_fp64=angular_fp64)
     checked = [i for members in dr.grid_groups().values() for i in members[:per_rung]]
     per = []
     t_ref = 0.0
@@ -346,20 +347,23 @@ def main(argv=None):
                          "one run per grid rung")
     ap.add_argument("--xc-frozen", action="store_true", help="exchange-correlation held at the ground state")
     ap.add_argument("--per-rung", type=int, default=1, help="--argon-ensemble-full: FP64 runs checked per rung")
+    ap.add_argument("--angular-fp64", action="store_true",
+                    help="the split form's angular products on the FP64 tensor cores (ggb_set_angular_fp64)")
     ap.add_argument("--sweep", action="store_true",
                     help="instead: FP64 self-sensitivity of argon LDA for dt in {0.02, 0.01, 0.005} and N_har "
                          "in {2, 3, 4} over the whole pulse")
     args = ap.parse_args(argv)
     if args.argon_ensemble_full:
         rep = compare_argon_ensemble_full(args.precision, angular=args.angular, xc_frozen=args.xc_frozen,
-                                          frozen=args.frozen, per_rung=args.per_rung)
+                                          frozen=args.frozen, per_rung=args.per_rung,
+                                          angular_fp64=args.angular_fp64)
         if args.out:
             with open(args.out, "w") as f:
                 f.write(json.dumps(rep) + "\n")
         print(json.dumps({k: v for k, v in rep.items() if k != "per_instance"}))
         return
     if args.hhe_ensemble:
-        rep = compare_hhe_ensemble(args.precision, angular=args.angular)
+        rep = compare_hhe_ensemble(args.precision, angular=args.angular, angular_fp64=args.angular_fp64)
         if args.out:
             with open(args.out, "w") as f:
                 f.write(json.dumps(rep) + "\n")
@@ -387,7 +391,7 @@ def main(argv=None):
         run = dataclasses.replace(run, xc_frozen=True, name=run.name + "-xcfrozen")
     if args.frozen:
         run = dataclasses.replace(run, use_hartree=0, name=run.name + "-frozen")
-    rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity)
+    rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64)
     line = json.dumps(rep)
     if args.out:
         with open(args.out, "w") as f:

@@ -75,17 +75,19 @@ __device__ double density_multipole(int L, int m, int n_l, const C* xs, int lane
 // The seven coefficient rows of one m (CF_CU .. CF_F3 order), contiguous: rows[c * n_l + l].
 // Density multipoles L = 0 .. n_den-1 of one orbital at the radius of this lane: the same terms and
 // literal l ranges as density_multipole, but every l loop is strided over the n_warps warps, and
-// this warp's partial sums are added to d[L] (the caller sums the warps).
+// this warp's partial sums are added to d[L] (the caller sums the warps).  Coefficient c of this m
+// is rows[c * row_stride + l] (row_stride 0: n_l, the rows contiguous).
 template <class C, int STRIDE>
 __device__ void density_partials(int n_den, int m, int n_l, const C* xs, int lane, const double* rows,
-                                 int warp, int n_warps, double (&d)[N_DEN]) {
-  const double* cu = rows + CF_CU * n_l;
-  const double* cd = rows + CF_CD * n_l;
-  const double* pp = rows + CF_P * n_l;
-  const double* qu = rows + CF_QU * n_l;
-  const double* qd = rows + CF_QD * n_l;
-  const double* p3 = rows + CF_P3 * n_l;
-  const double* f3 = rows + CF_F3 * n_l;
+                                 int warp, int n_warps, double (&d)[N_DEN], int row_stride = 0) {
+  const size_t rs = row_stride > 0 ? (size_t)row_stride : (size_t)n_l;
+  const double* cu = rows + CF_CU * rs;
+  const double* cd = rows + CF_CD * rs;
+  const double* pp = rows + CF_P * rs;
+  const double* qu = rows + CF_QU * rs;
+  const double* qd = rows + CF_QD * rs;
+  const double* p3 = rows + CF_P3 * rs;
+  const double* f3 = rows + CF_F3 * rs;
   auto X = [&](int a, int b) { return xdot<C, STRIDE>(xs, n_l, a, b, lane); };
   // L = 0
   for (int lp = m + warp; lp < n_l; lp += n_warps) d[0] += X(lp, lp);

@@ -533,7 +533,9 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     // (each CTA streams the chain matrices once per product: fewer radii per CTA cost more of that
     // traffic than the extra CTAs gain, measured for the FP64 form), the int8 form 16 when N_l > 128
     // (two M tiles of channels)
-    g.obs_seg = (dims->precision == GGB_SPLIT_INT8 && g.d.n_l > 128) ? 16 : TR;
+    // radii per observables partial = the angular tile: 16 for the FP64 form and for the int8 form
+    // with two channel tiles (N_l > 128), 32 otherwise
+    g.obs_seg = (dims->precision == GGB_FP64 || (dims->precision == GGB_SPLIT_INT8 && g.d.n_l > 128)) ? 16 : TR;
     g.n_tiles = (g.d.n_r + g.obs_seg - 1) / g.obs_seg;
     g.ldS = ((g.d.n_l + 7) / 8) * 8;
   }
@@ -740,6 +742,16 @@ int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages) {
     return fail(ctx, GGB_ERR_ARG, "radial_stages %d outside 2..8", radial_stages);
   ctx->groups[group].mixed.i8.tune_bn = radial_bn;
   ctx->groups[group].mixed.i8.tune_stages = radial_stages;
+  return GGB_OK;
+}
+
+int ggb_set_angular_fp64(ggb_ctx* ctx, int group, int on) {
+  if (!ctx) return GGB_ERR_ARG;
+  if (group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, GGB_ERR_ARG, "group %d out of range", group);
+  if (ctx->dims.precision != GGB_SPLIT_INT8)
+    return fail(ctx, GGB_ERR_STATE, "ggb_set_angular_fp64 applies to the split_int8 form only");
+  if (ctx->prepared) return fail(ctx, GGB_ERR_STATE, "ggb_set_angular_fp64 after the first ggb_step");
+  ctx->groups[group].mixed.angular_fp64 = on != 0;
   return GGB_OK;
 }
 

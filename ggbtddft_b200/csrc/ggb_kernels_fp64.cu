@@ -1,13 +1,14 @@
 // FP64 (parity form) kernels of the split-operator step.
 //
-//  k_angular_fp64  one half of the angular step for a tile of 32 radii of one orbital column:
+//  k_angular_fp64  one half of the angular step for a tile of 16 radii of one orbital column:
 //                  the whole l-vector of every radius is held in shared memory while the chain
 //                  (rotate -> phase -> [pre-multiplied rotate pair] -> phase ... -> rotate back,
-//                  plus the l-diagonal S phase) is applied.  Replaces, per half-step, the 3
-//                  launches of each of h_couplingFF/FP/D/P (couplingP.cuh:108-125, couplingD.cuh,
-//                  couplingF.cuh) and h_couplingS (couplingS.cuh:43-57).  The second half also
-//                  produces the density-multipole and dipole/acceleration partial sums of the new
-//                  orbitals (hartreePotentialDensity.cuh:1-181, dipoleMoment.cuh:1-75,
+//                  plus the l-diagonal S phase) is applied, each product on the FP64 tensor cores
+//                  (mma.sync m8n8k4).  Replaces, per half-step, the 3 launches of each of
+//                  h_couplingFF/FP/D/P (couplingP.cuh:108-125, couplingD.cuh, couplingF.cuh) and
+//                  h_couplingS (couplingS.cuh:43-57).  The second half also produces the
+//                  density-multipole and dipole/acceleration partial sums of the new orbitals
+//                  (hartreePotentialDensity.cuh:1-181, dipoleMoment.cuh:1-75,
 //                  dipoleAcceleration.cuh:1-71), so the orbitals are read once per half-step.
 //  k_radial_fp64   x_l <- A_l x_l for every l with A_l(a,b) = W[l][b][a]: the batched ZGEMM of
 //                  h_propagationH0 (h_timePropagation.cuh:1-30), out of place.  Persistent, two CTAs
@@ -20,8 +21,6 @@
 //                  (occupation-weighted sum over orbitals), Hartree potentials by compensated
 //                  prefix scans (h_calculateHartreePotential.cuh:1-136), LDA exchange
 //                  (h_calculateExchangeCorrelationPotential.cuh:1-56), step counter.
-#include <cooperative_groups.h>
-
 #include <algorithm>
 #include <cstdio>
 #include "ggb_internal.cuh"
@@ -35,199 +34,247 @@ namespace ggb {
 // angular chain
 // ---------------------------------------------------------------------------------------------
 
-constexpr int ANG_JB = 8;   // eigen-channels j per register block
+// A tile is RT radii of one orbital column (RT = the group's observables segment: 16 for the FP64
+// form, 16 or 32 for the initial partials of the int8 form): the whole l-vector of each radius sits
+// in shared memory as a [rows][2 RT + 8] FP64 matrix (column 2 rad + 0/1 = real/imaginary part of
+// radius rad; rows N_l rounded up to 8, zero beyond N_l), and every product of the chain
+// y_j = sum_l S[l][j] x_l is a small real GEMM  Y (N_l x 2 RT) = S^T (N_l x N_l) X (N_l x 2 RT)  on
+// the FP64 tensor cores: mma.sync m8n8k4 (8 channels x 8 columns x 4 l per instruction).  Each warp
+// owns pairs of 8-channel tiles (16 j) over all 2 RT columns; its S fragments come from L2
+// (read-only path), prefetched one chunk of AM_KU k-steps ahead; its X fragments from shared
+// memory.  The phases are applied to the accumulators in registers (each thread holds whole complex
+// numbers: the real and imaginary column of one radius), then written to the other buffer for the
+// next product.
+constexpr int AM_WARPS = 4;
+constexpr int AM_KU = 4;                    // k-steps (4 l each) per prefetch chunk
+// row stride in doubles: +8 puts the 4 rows of an X fragment on alternating bank halves
+__host__ __device__ constexpr int angular_ldx(int rt) { return 2 * rt + 8; }
 
-// RT radii per CTA (32, or 16 with the two half-warps on different eigen-channel blocks): lane % RT is
-// the radius, lane / RT picks the half; the group's observables partials cover RT radii each.
-// CL = 2: a cluster of two CTAs shares one tile: each computes half of the eigen-channels of every
-// product (reading half of the chain matrix) and writes its half into both CTAs' shared memory
-// (distributed shared memory), a cluster barrier between products; the same arithmetic as CL = 1,
-// with twice the CTAs for runs too small to fill the GPU.
-template <int RT, int CL>
-__global__ void __launch_bounds__(ANG_WARPS * 32)
-k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* __restrict__ xout, int do_obs) {
-  namespace cg = cooperative_groups;
-  constexpr int SUB = 32 / RT;                    // lanes groups per warp (1 or 2)
-  constexpr int NSUB = ANG_WARPS * SUB;           // thread groups that stride l and j in one CTA
-  extern __shared__ double2 sm[];  // two [N_l][RT] buffers
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int lr = lane % RT;                       // radius of this lane
-  const int sub = warp * SUB + lane / RT;         // this thread's group
-  const int crank = CL == 2 ? (int)cg::this_cluster().block_rank() : 0;
-  const int gsub = crank * NSUB + sub;            // this thread's group across the cluster
-  const int tilesN = (g.n_r + RT - 1) / RT;
-  const int bt = blockIdx.x / CL;                 // the tile of this CTA (or CTA pair)
-  const int col = bt / tilesN;
-  const int tile = bt - col * tilesN;
-  const int r = tile * RT + lr;
-  const bool rv = r < g.n_r;
+__host__ __device__ constexpr int angular_rows_mma(int n_l) {
+  // N_l rounded up to 8 (the channel tiles), and at least 16 rows: the free buffer holds the
+  // AM_NSUB x N_DEN x AM_RT density partials of the epilogue
+  return ((n_l + 7) / 8 * 8) > 16 ? (n_l + 7) / 8 * 8 : 16;
+}
+
+__device__ __forceinline__ void mma_f64_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// One half of the angular step (or, with the empty chain of half 2, only the epilogue): replaces,
+// per half-step, the 3 launches of each of h_couplingFF/FP/D/P (couplingP.cuh:108-125,
+// couplingD.cuh, couplingF.cuh) and h_couplingS (couplingS.cuh:43-57); the second half also
+// produces the density-multipole and dipole/acceleration partial sums of the new orbitals
+// (hartreePotentialDensity.cuh:1-181, dipoleMoment.cuh:1-75, dipoleAcceleration.cuh:1-71).
+template <int RT>
+__global__ void __launch_bounds__(AM_WARPS * 32)
+k_angular_fp64(GroupArgs g, int half, const double2* __restrict__ xin, double2* xout, int do_obs) {
+  constexpr int AM_RT = RT;
+  constexpr int AM_LDX = angular_ldx(RT);
+  constexpr int AM_NT = 2 * RT / 8;                  // 8-column tiles per row
+  constexpr int AM_NSUB = AM_WARPS * 32 / RT;        // lane groups of RT threads (epilogue)
+  extern __shared__ double smd[];
+  __shared__ double s_rr[RT], s_rE[RT], s_v1[RT], s_v2[RT], s_v3[RT], s_sb[RT];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int gid = lane >> 2;      // fragment row group
+  const int q = lane & 3;         // fragment thread in group
   const int n_l = g.n_l;
-  double2* xs = sm;
-  double2* ys = sm + (size_t)n_l * RT;
+  const int rows = angular_rows_mma(n_l);
+  const int tilesN = (g.n_r + AM_RT - 1) / AM_RT;
+  const int col = blockIdx.x / tilesN;
+  const int tile = blockIdx.x - col * tilesN;
+  const int r0 = tile * AM_RT;
+  double* xs = smd;
+  double* ys = smd + (size_t)rows * AM_LDX;
   const int m = g.col_m[col];
   const RunDev run = g.runs[g.col_run[col]];
   int step = *g.step;
   if (step >= run.n_t) step = run.n_t - 1;  // overflow is flagged by k_finalize
 
-  for (int l = sub; l < n_l; l += NSUB)
-    xs[l * RT + lr] = rv ? xin[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
-
+  // the tile's orbitals (zero beyond N_l and beyond N_r), zero padding rows in both buffers
+  for (int i = tid; i < rows * AM_RT; i += blockDim.x) {
+    const int l = i / AM_RT, rad = i - l * AM_RT, r = r0 + rad;
+    const double2 v = (l < n_l && r < g.n_r) ? xin[((size_t)l * g.n_cols + col) * g.n_r + r]
+                                             : make_double2(0.0, 0.0);
+    *reinterpret_cast<double2*>(xs + (size_t)l * AM_LDX + 2 * rad) = v;
+    if (l >= n_l) *reinterpret_cast<double2*>(ys + (size_t)l * AM_LDX + 2 * rad) = make_double2(0.0, 0.0);
+  }
   // per-radius potentials
-  const double rr = rv ? g.r[r] : 1.0;
-  const int rc = rv ? r : 0;
-  const double E = run.E[step];
-  double v1 = 0.0, v2 = 0.0, v3 = 0.0, sbase = 0.0;
-  if (g.hartree_on) {
-    v1 = run.v[1 * g.n_r + rc];
-    v2 = run.v[2 * g.n_r + rc];
-    v3 = run.v[3 * g.n_r + rc];
-    // couplingS.cuh:20-21, evaluated left to right
-    sbase = run.v[rc] - run.v0[rc] + run.vexc[rc] - run.vexc0[rc];
+  if (tid < AM_RT) {
+    const int r = r0 + tid;
+    const bool rv = r < g.n_r;
+    const int rc = rv ? r : 0;
+    const double rr = rv ? g.r[r] : 1.0;
+    double v1 = 0.0, v2 = 0.0, v3 = 0.0, sbase = 0.0;
+    if (g.hartree_on) {
+      v1 = run.v[1 * g.n_r + rc];
+      v2 = run.v[2 * g.n_r + rc];
+      v3 = run.v[3 * g.n_r + rc];
+      // couplingS.cuh:20-21, evaluated left to right
+      sbase = run.v[rc] - run.v0[rc] + run.vexc[rc] - run.vexc0[rc];
+    }
+    s_rr[tid] = rr;
+    s_rE[tid] = rr * run.E[step];
+    s_v1[tid] = v1;
+    s_v2[tid] = v2;
+    s_v3[tid] = v3;
+    s_sb[tid] = sbase;
   }
   const double hdt = 0.5 * g.dt;
   const double* pco = g.coef + ((size_t)CF_P * g.n_m + m) * n_l;
-  if constexpr (CL == 2) cg::this_cluster().sync();   // both CTAs running before any remote write
-  else __syncthreads();
+  __syncthreads();
 
   const Chain& ch = g.chain[half];
   if (ch.pre_s) {
-    for (int l = sub; l < n_l; l += NSUB) {
-      double eta = sbase + pco[l] * v2;
+    for (int i = tid; i < n_l * AM_RT; i += blockDim.x) {
+      const int l = i / AM_RT, rad = i - l * AM_RT;
+      double eta = s_sb[rad] + pco[l] * s_v2[rad];
       eta *= hdt;
-      xs[l * RT + lr] = cmul_conj_phase(xs[l * RT + lr], eta);
+      double2* p = reinterpret_cast<double2*>(xs + (size_t)l * AM_LDX + 2 * rad);
+      *p = cmul_conj_phase(*p, eta);
     }
     __syncthreads();
   }
 
+  const int k_steps = (n_l + 3) / 4;
+  const int n_pairs = ((n_l + 7) / 8 + 1) / 2;
   for (int o = 0; o < ch.n_ops; ++o) {
     const ChainOp op = ch.ops[o];
     const double* S = g.mats + ((size_t)op.mat * g.n_m + m) * (size_t)n_l * g.ldS;
     const bool last = (o == ch.n_ops - 1);
-    double base = 0.0;
-    if (op.phase == PH_P) base = g.p_hartree ? (rr * E + v1) : (rr * E);
-    else if (op.phase == PH_D) base = v2;
-    else if (op.phase != PH_NONE) base = v3;  // FP and FF
     const double* Dv = g.dph + ((size_t)op.coupling * g.n_m + m) * g.ldS;
-    double2* ys_peer = ys;
-    if constexpr (CL == 2) ys_peer = cg::this_cluster().map_shared_rank(ys, crank ^ 1);
-    for (int j0 = gsub * ANG_JB; j0 < n_l; j0 += CL * NSUB * ANG_JB) {
-      double2 acc[ANG_JB];
+    for (int pr = warp; pr < n_pairs; pr += AM_WARPS) {
+      const int ja = pr * 16 + gid, jb = ja + 8;
+      const bool va = ja < n_l, vb = jb < n_l;
+      double acc[2][AM_NT][2];
 #pragma unroll
-      for (int q = 0; q < ANG_JB; ++q) acc[q] = make_double2(0.0, 0.0);
-      const double* Sc = S + j0;
-      int l = m;
-      // four l rows per iteration: 16 independent 16-byte loads of S in flight per thread
-      for (; l + 4 <= n_l; l += 4) {
-        double2 sv[4][ANG_JB / 2];
-        double2 xv[4];
+      for (int t = 0; t < 2; ++t)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          xv[u] = xs[(l + u) * RT + lr];
-          const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)(l + u) * g.ldS);
+        for (int nt = 0; nt < AM_NT; ++nt) acc[t][nt][0] = acc[t][nt][1] = 0.0;
+      // S fragments (A = S^T: row j, column l) of AM_KU k-steps; rows l < m are skipped, as the
+      // reference's couplings start at l = m
+      double fa[AM_KU][2], fn[AM_KU][2];
+      auto load_a = [&](int ks0, double (&dst)[AM_KU][2]) {
 #pragma unroll
-          for (int h = 0; h < ANG_JB / 2; ++h) sv[u][h] = __ldg(Srow + h);
+        for (int u = 0; u < AM_KU; ++u) {
+          const int l = (ks0 + u) * 4 + q;
+          const bool lv = l >= m && l < n_l;
+          dst[u][0] = (lv && va) ? __ldg(S + (size_t)l * g.ldS + ja) : 0.0;
+          dst[u][1] = (lv && vb) ? __ldg(S + (size_t)l * g.ldS + jb) : 0.0;
         }
+      };
+      load_a(0, fa);
+      for (int ks0 = 0; ks0 < k_steps; ks0 += AM_KU) {
+        load_a(ks0 + AM_KU, fn);   // past the last k-step it loads nothing (l >= N_l)
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < AM_KU; ++u) {
+          if (ks0 + u < k_steps) {
+            const double* xr = xs + (size_t)((ks0 + u) * 4 + q) * AM_LDX + gid;
+            double fb[AM_NT];
 #pragma unroll
-          for (int h = 0; h < ANG_JB / 2; ++h) {
-            acc[2 * h].x += sv[u][h].x * xv[u].x;     acc[2 * h].y += sv[u][h].x * xv[u].y;
-            acc[2 * h + 1].x += sv[u][h].y * xv[u].x; acc[2 * h + 1].y += sv[u][h].y * xv[u].y;
+            for (int nt = 0; nt < AM_NT; ++nt) fb[nt] = xr[nt * 8];
+#pragma unroll
+            for (int nt = 0; nt < AM_NT; ++nt) {
+              mma_f64_8x8x4(acc[0][nt][0], acc[0][nt][1], fa[u][0], fb[nt]);
+              mma_f64_8x8x4(acc[1][nt][0], acc[1][nt][1], fa[u][1], fb[nt]);
+            }
           }
-      }
-      for (; l < n_l; ++l) {
-        const double2 xv = xs[l * RT + lr];
-        const double2* Srow = reinterpret_cast<const double2*>(Sc + (size_t)l * g.ldS);
-#pragma unroll
-        for (int h = 0; h < ANG_JB / 2; ++h) {
-          const double2 sv = __ldg(Srow + h);
-          acc[2 * h].x += sv.x * xv.x;     acc[2 * h].y += sv.x * xv.y;
-          acc[2 * h + 1].x += sv.y * xv.x; acc[2 * h + 1].y += sv.y * xv.y;
         }
-      }
 #pragma unroll
-      for (int q = 0; q < ANG_JB; ++q) {
-        const int j = j0 + q;
-        if (j < n_l) {
-          double2 y = acc[q];
-          // phase in the eigenbasis (couplingP.cuh:61-106 and twins)
+        for (int u = 0; u < AM_KU; ++u) { fa[u][0] = fn[u][0]; fa[u][1] = fn[u][1]; }
+      }
+      // phases on the accumulators: thread (gid, q) holds channel j = pair base + 8 t + gid, radius
+      // 4 nt + q, real and imaginary part (couplingP.cuh:61-106 and twins)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int j = pr * 16 + 8 * t + gid;
+        if (j >= n_l) continue;
+        const double dj = Dv[j];
+#pragma unroll
+        for (int nt = 0; nt < AM_NT; ++nt) {
+          const int rad = 4 * nt + q;
+          double2 y = make_double2(acc[t][nt][0], acc[t][nt][1]);
           if (op.phase == PH_THETA && j >= m) {
             // the theta form: the whole angular potential at node x_j
-            const double xj = Dv[j];
-            double eta = (rr * E + v1) * xj + v2 * legendre_p2(xj) + v3 * legendre_p3(xj) + sbase;
+            double eta = (s_rE[rad] + s_v1[rad]) * dj + s_v2[rad] * legendre_p2(dj) +
+                         s_v3[rad] * legendre_p3(dj) + s_sb[rad];
             // n_har > 4: the multipoles L >= 1 at this node come from the exact-quadrature table
-            if (g.theta_tab && rv) eta += run.htab[((size_t)m * n_l + j) * g.n_r + r];
+            if (g.theta_tab && r0 + rad < g.n_r) eta += run.htab[((size_t)m * n_l + j) * g.n_r + r0 + rad];
             eta *= hdt;
             y = cmul_conj_phase(y, eta);
           } else if (op.phase != PH_NONE && j >= m) {
-            double eta = base;
-            eta *= hdt * Dv[j];
+            double eta;
+            if (op.phase == PH_P) eta = g.p_hartree ? (s_rE[rad] + s_v1[rad]) : s_rE[rad];
+            else if (op.phase == PH_D) eta = s_v2[rad];
+            else eta = s_v3[rad];   // FP and FF
+            eta *= hdt * dj;
             y = cmul_conj_phase(y, eta);
           }
           if (last && ch.post_s) {
-            double eta = sbase + pco[j] * v2;
+            double eta = s_sb[rad] + pco[j] * s_v2[rad];
             eta *= hdt;
             y = cmul_conj_phase(y, eta);
           }
-          ys[j * RT + lr] = y;
-          if constexpr (CL == 2) ys_peer[j * RT + lr] = y;
+          *reinterpret_cast<double2*>(ys + (size_t)j * AM_LDX + 2 * rad) = y;
         }
       }
     }
-    if constexpr (CL == 2) cg::this_cluster().sync();
-    else __syncthreads();
-    double2* t = xs; xs = ys; ys = t;
+    __syncthreads();
+    double* t = xs; xs = ys; ys = t;
   }
 
-  // both CTAs of a pair hold the whole result: each writes and reduces its share of l
-  if (rv && xout)
-    for (int l = gsub; l < n_l; l += CL * NSUB) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = xs[l * RT + lr];
+  const double2* x2 = reinterpret_cast<const double2*>(xs);
+  if (xout)
+    for (int i = tid; i < n_l * AM_RT; i += blockDim.x) {
+      const int l = i / AM_RT, rad = i - l * AM_RT, r = r0 + rad;
+      if (r < g.n_r) xout[((size_t)l * g.n_cols + col) * g.n_r + r] = x2[(size_t)l * (AM_LDX / 2) + rad];
+    }
 
   if (do_obs) {
-    const double fr2 = rv ? pow(rr, -2.0) : 0.0;
-    observables_tile<double2, RT>(g, xs, col, m, tile * RT, lr, gsub, CL * NSUB, rr, fr2);
+    // lane groups of AM_RT threads, one radius per thread
+    const int lr = lane % AM_RT, sub = warp * (32 / AM_RT) + lane / AM_RT;
+    const double rr = s_rr[lr];
+    const double fr2 = (r0 + lr < g.n_r) ? pow(rr, -2.0) : 0.0;
+    observables_tile<double2, AM_LDX / 2>(g, x2, col, m, r0, lr, sub, AM_NSUB, rr, fr2);
+    // density multipoles: the literal l loops strided over the lane groups, then the groups summed
+    // in order (the free buffer holds the AM_NSUB x N_DEN x AM_RT partials)
     const int n_den = g.n_den > 0 ? g.n_den : 1;  // L = 0 is always needed for the norm
-    for (int L = gsub; L < n_den; L += CL * NSUB) {
-      const double d = density_multipole<double2, RT>(L, m, n_l, xs, lr, g.coef, g.n_m);
-      if (rv) g.dens[((size_t)col * N_DEN + L) * g.n_r + r] = d;
+    double d[N_DEN] = {0.0, 0.0, 0.0, 0.0};
+    density_partials<double2, AM_LDX / 2>(n_den, m, n_l, x2, lr, g.coef + (size_t)m * n_l, sub, AM_NSUB, d,
+                                          g.n_m * n_l);
+#pragma unroll
+    for (int L = 0; L < N_DEN; ++L) ys[(sub * N_DEN + L) * AM_RT + lr] = d[L];
+    __syncthreads();
+    if (tid < n_den * AM_RT) {
+      const int L = tid / AM_RT, p = tid - L * AM_RT, rl = r0 + p;
+      double sum = 0.0;
+      for (int w = 0; w < AM_NSUB; ++w) sum += ys[(w * N_DEN + L) * AM_RT + p];
+      if (rl < g.n_r) g.dens[((size_t)col * N_DEN + L) * g.n_r + rl] = sum;
     }
   }
 }
 
-size_t angular_smem_fp64(int n_l) { return 2 * (size_t)n_l * TR * sizeof(double2); }
-
-static int g_angular_sms = 148;
-
-template <int RT>
-static void launch_angular_rt(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
-                              cudaStream_t s) {
-  const int tiles = g.n_cols * ((g.n_r + RT - 1) / RT);
-  const size_t smem = 2 * (size_t)g.n_l * RT * sizeof(double2);
-  if (tiles >= 2 * g_angular_sms) {
-    k_angular_fp64<RT, 1><<<tiles, ANG_WARPS * 32, smem, s>>>(g, half, xin, xout, do_obs);
-    return;
-  }
-  // too few tiles to fill the GPU: a CTA pair per tile
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(2 * tiles);
-  cfg.blockDim = dim3(ANG_WARPS * 32);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = 2;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_angular_fp64<RT, 2>, g, half, xin, xout, do_obs);
+static size_t angular_smem_rt(int n_l, int rt) {
+  return 2 * (size_t)angular_rows_mma(n_l) * angular_ldx(rt) * sizeof(double);
+}
+// the largest launch for groups of up to n_l channels: 32-radius tiles only for N_l <= 128 (the int8
+// form's initial partials), 16-radius tiles otherwise
+size_t angular_smem_fp64(int n_l) {
+  return std::max(angular_smem_rt(std::min(n_l, 128), TR), angular_smem_rt(n_l, 16));
 }
 
 void launch_angular_fp64(const GroupArgs& g, int half, const double2* xin, double2* xout, int do_obs,
                          cudaStream_t s) {
-  if (g.obs_seg == 16) launch_angular_rt<16>(g, half, xin, xout, do_obs, s);
-  else launch_angular_rt<TR>(g, half, xin, xout, do_obs, s);
+  if (g.obs_seg == 16) {
+    const int tiles = g.n_cols * ((g.n_r + 15) / 16);
+    k_angular_fp64<16><<<tiles, AM_WARPS * 32, angular_smem_rt(g.n_l, 16), s>>>(g, half, xin, xout, do_obs);
+  } else {
+    const int tiles = g.n_cols * ((g.n_r + TR - 1) / TR);
+    k_angular_fp64<TR><<<tiles, AM_WARPS * 32, angular_smem_rt(g.n_l, TR), s>>>(g, half, xin, xout, do_obs);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -665,15 +712,9 @@ cudaError_t configure_kernels_fp64(int n_l_max, int n_r_max) {
   if (e != cudaSuccess) return e;
   if (angular_smem_fp64(n_l_max) > (size_t)optin || 3 * (size_t)n_r_max * sizeof(double) > (size_t)optin)
     return cudaErrorInvalidValue;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR, 1>, optin);
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<16>, optin);
   if (e != cudaSuccess) return e;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<16, 1>, optin);
-  if (e != cudaSuccess) return e;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR, 2>, optin);
-  if (e != cudaSuccess) return e;
-  e = set_max_dynamic_smem((const void*)k_angular_fp64<16, 2>, optin);
-  if (e != cudaSuccess) return e;
-  e = cudaDeviceGetAttribute(&g_angular_sms, cudaDevAttrMultiProcessorCount, dev);
+  e = set_max_dynamic_smem((const void*)k_angular_fp64<TR>, optin);
   if (e != cudaSuccess) return e;
   e = configure_radial_fp64();
   if (e != cudaSuccess) return e;

@@ -787,10 +787,13 @@ void mixed_init(MixedGroup& m, const GroupArgs& a, const double2*, cudaStream_t 
 static void angular_half(MixedGroup& m, const GroupArgs& a, int half, cudaStream_t s) {
   if (m.precision == GGB_SPLIT_INT8) {
     if (half == 0) {
-      int8_angular(m, a, 0, m.Xd, m.Xd, s);
+      if (m.angular_fp64) launch_angular_fp64(a, 0, m.Xd, m.Xd, 0, s);
+      else int8_angular(m, a, 0, m.Xd, m.Xd, s);
       int8_slice_x(m, a, m.Xd, s);
     } else {
-      int8_angular(m, a, 1, m.Yd, m.Xd, s);   // also the density and dipole partial sums
+      // also the density and dipole partial sums
+      if (m.angular_fp64) launch_angular_fp64(a, 1, m.Yd, m.Xd, 1, s);
+      else int8_angular(m, a, 1, m.Yd, m.Xd, s);
     }
     return;
   }

@@ -54,6 +54,9 @@ struct MixedGroup {
   float* mats_f = nullptr;          // chain matrices in FP32
   CUtensorMap tmW;
   CUtensorMap tmX;
+  // int8 form: the angular products on the FP64 tensor cores (the FP64 form's kernel, mma.sync f64)
+  // instead of int8 slices on tcgen05; the radial product stays int8
+  bool angular_fp64 = false;
   // tensor-core angular chain
   bool angular_tc = false;
   __nv_bfloat16* St = nullptr;      // S^T planes [mat][m][hi,lo][m_tiles*128 (j)][k_atoms*64 (l)]

@@ -4,6 +4,8 @@
 //
 //  k_peak_fp64  eight independent FMA chains per thread, every SM filled with 8 x 256 threads:
 //               2 flops per DFMA, nothing else issued in the loop.
+//  k_peak_dmma  eight independent mma.sync m8n8k4 f64 accumulators per warp, the same grid as
+//               k_peak_fp64: 2 * 8 * 8 * 4 flops per MMA.
 //  k_peak_i8    one CTA per SM (its shared-memory request leaves no room for a second); one
 //               thread issues back-to-back M = 128, N = 256, K = 32 int8 MMAs from two tiles (K-major, 32-byte swizzle, pseudo-random bytes) into
 //               one tensor-memory accumulator, then commits once: 2 * 128 * 256 * 32 ops per MMA.
@@ -45,6 +47,27 @@ __global__ void __launch_bounds__(PK_FMA_THREADS) k_peak_fp64(int iters, double 
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < PK_FMA_CHAINS; ++k) s += a[k];
+  if (s == -1.0) g_peak_sink = s;   // never true; keeps the chains live
+}
+
+__global__ void __launch_bounds__(PK_FMA_THREADS) k_peak_dmma(int iters, double seed) {
+  double c[PK_FMA_CHAINS][2];
+#pragma unroll
+  for (int k = 0; k < PK_FMA_CHAINS; ++k) {
+    c[k][0] = seed + k;
+    c[k][1] = seed - k;
+  }
+  const double a = 1.0 - 1e-13 * (threadIdx.x & 7), b = 1e-3;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < PK_FMA_CHAINS; ++k)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                   : "+d"(c[k][0]), "+d"(c[k][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < PK_FMA_CHAINS; ++k) s += c[k][0] + c[k][1];
   if (s == -1.0) g_peak_sink = s;   // never true; keeps the chains live
 }
 
@@ -153,5 +176,36 @@ extern "C" int ggb_measure_peaks(double* fp64_tflops, double* int8_tops, void* s
   const double mma_ops = 2.0 * PK_MMA_M * PK_MMA_N * PK_MMA_K * (double)n_mma * sms;
   if (fp64_tflops) *fp64_tflops = fma_flops / (best_f * 1e-3) / 1e12;
   if (int8_tops) *int8_tops = mma_ops / (best_i * 1e-3) / 1e12;
+  return GGB_OK;
+}
+
+extern "C" int ggb_measure_peak_fp64_mma(double* tflops, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return GGB_ERR_CUDA;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GGB_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return GGB_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return GGB_ERR_CUDA;
+  }
+  const int iters = 1 << 13, reps = 3;
+  float best = 1e30f, ms = 0.0f;
+  for (int r = 0; r < reps + 1; ++r) {   // the first launch is a warm-up
+    cudaEventRecord(e0, s);
+    k_peak_dmma<<<sms * PK_FMA_BLOCKS_PER_SM, PK_FMA_THREADS, 0, s>>>(iters, 1.0);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms < best) best = ms;
+  }
+  const cudaError_t err = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return GGB_ERR_CUDA;
+  const double warps = (double)sms * PK_FMA_BLOCKS_PER_SM * (PK_FMA_THREADS / 32);
+  const double flops = 2.0 * 8 * 8 * 4 * PK_FMA_CHAINS * (double)iters * warps;
+  if (tflops) *tflops = flops / (best * 1e-3) / 1e12;
   return GGB_OK;
 }

@@ -54,7 +54,8 @@ _lib = None
 EXPORTS = ("ggb_create", "ggb_set_grid", "ggb_set_radial_propagators", "ggb_set_angular", "ggb_set_orbitals",
            "ggb_set_field", "ggb_step", "ggb_get_step", "ggb_get_observables", "ggb_get_orbitals",
            "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase",
-           "ggb_set_tuning", "ggb_observables_noalloc", "ggb_measure_peaks")
+           "ggb_set_tuning", "ggb_observables_noalloc", "ggb_measure_peaks", "ggb_measure_peak_fp64_mma",
+           "ggb_set_angular_fp64")
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -79,6 +80,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_get_step": ([P, ctypes.POINTER(ctypes.c_int)], I_),
         "ggb_launch_phase": ([P, I_, P], I_),
         "ggb_set_tuning": ([P, I_, I_, I_], I_),
+        "ggb_set_angular_fp64": ([P, I_, I_], I_),
         "ggb_get_observables": ([P, I_, P, P, P, I_, I_], I_),
         "ggb_get_orbitals": ([P, I_, P], I_),
         "ggb_get_potentials": ([P, I_, P, P, P, P], I_),
@@ -87,6 +89,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_version": ([], ctypes.c_char_p),
         "ggb_observables_noalloc": ([P, P, P, I_, I_, I_, P, P, P, P], I_),
         "ggb_measure_peaks": ([ctypes.POINTER(D), ctypes.POINTER(D), P], I_),
+        "ggb_measure_peak_fp64_mma": ([ctypes.POINTER(D), P], I_),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -105,13 +108,19 @@ def _c(a, dtype):
 
 
 def measure_peaks(stream: Optional[int] = None) -> Dict[str, float]:
-    """FP64 FMA (TFLOP/s) and tcgen05 int8 (TOP/s) peaks of the current GPU (ggb_measure_peaks)."""
+    """Peaks of the current GPU from the library's microbenchmarks: FP64 FMA and FP64 mma.sync
+    (TFLOP/s; ``fp64_tflops`` is the larger, the FP64 roofline) and tcgen05 int8 (TOP/s)."""
     lib = load_library()
-    f, i = ctypes.c_double(), ctypes.c_double()
-    rc = lib.ggb_measure_peaks(ctypes.byref(f), ctypes.byref(i), ctypes.c_void_p(stream) if stream else None)
+    f, i, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    h = ctypes.c_void_p(stream) if stream else None
+    rc = lib.ggb_measure_peaks(ctypes.byref(f), ctypes.byref(i), h)
     if rc != 0:
         raise GGBError(f"ggb_measure_peaks failed: {rc}")
-    return dict(fp64_tflops=f.value, int8_tops=i.value)
+    rc = lib.ggb_measure_peak_fp64_mma(ctypes.byref(d), h)
+    if rc != 0:
+        raise GGBError(f"ggb_measure_peak_fp64_mma failed: {rc}")
+    return dict(fp64_tflops=max(f.value, d.value), fp64_fma_tflops=f.value, fp64_mma_tflops=d.value,
+                int8_tops=i.value)
 
 
 def group_runs(runs: Sequence[RunInputs]) -> List[List[int]]:
@@ -132,10 +141,12 @@ class TimePropagation:
 
     def __init__(self, runs: Sequence[RunInputs], precision: str = "fp64", per_l: bool = True,
                  n_t: Optional[int] = None, groups: Optional[List[List[int]]] = None, W_device=None,
-                 tuning: Optional[Dict[int, Tuple[int, int]]] = None, autotune: bool = False):
+                 tuning: Optional[Dict[int, Tuple[int, int]]] = None, autotune: bool = False,
+                 angular_fp64: bool = False):
         """``tuning`` = {group: (radial_bn, radial_stages)} (ggb_set_tuning); ``autotune`` = True
         takes each group's tiles from the autotuner's cache, timing the candidates on a miss
-        (split_int8 form only)."""
+        (split_int8 form only); ``angular_fp64`` = True runs the split_int8 form's angular products
+        on the FP64 tensor cores (ggb_set_angular_fp64), the radial product staying int8."""
         self.lib = load_library()
         self.runs = list(runs)
         self.precision = precision
@@ -180,6 +191,10 @@ class TimePropagation:
                                _ptr(_c(r0.D[c][m], np.float64)))
         for gi, (bn, stages) in (tuning or {}).items():
             self._call("ggb_set_tuning", int(gi), int(bn), int(stages))
+        self.angular_fp64 = bool(angular_fp64) and precision == "split_int8"
+        if self.angular_fp64:
+            for gi in range(len(self.groups)):
+                self._call("ggb_set_angular_fp64", gi, 1)
         for i in range(len(self.runs)):
             self.set_orbitals(i, self.runs[i].x0)
             self.set_field(i, self.runs[i].E)

@@ -146,6 +146,13 @@ int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream);
    reference (its radial product is a cuBLAS call). */
 int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages);
 
+/* split_int8 form, before the first ggb_step: on = 1 runs the angular products of `group` on the FP64
+   tensor cores (the FP64 form's kernel: mma.sync m8n8k4 f64, FP64 S matrices and phases) instead of as
+   int8 slice products on tcgen05; the radial product stays int8.  The angular step is then exact in
+   FP64 (the int8 form's angular operands carry 31 bits).  GGB_ERR_STATE for other forms or after the
+   first step.  No counterpart in the reference. */
+int ggb_set_angular_fp64(ggb_ctx* ctx, int group, int on);
+
 /* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */
 int ggb_get_step(ggb_ctx* ctx, int* step);
 
@@ -195,6 +202,12 @@ int ggb_observables_noalloc(const double* x, const double* r, const int* m, int 
    `stream`, a few tens of milliseconds.  These are the denominators of the roofline fractions of the
    FP64 and int8 forms.  No counterpart in the reference. */
 int ggb_measure_peaks(double* fp64_tflops, double* int8_tops, void* stream);
+
+/* Peak FP64 throughput of the current GPU's tensor cores in TFLOP/s, measured with the library's own
+   kernel: independent chains of mma.sync m8n8k4 f64 in every warp of a full GPU (the instruction
+   the FP64 form's angular products use).  Synchronous on `stream`.  The FP64 roofline takes the
+   larger of this and the FMA figure of ggb_measure_peaks.  No counterpart in the reference. */
+int ggb_measure_peak_fp64_mma(double* tflops, void* stream);
 
 /* Library version string. */
 const char* ggb_version(void);

@@ -193,3 +193,28 @@ def test_fp64_frozen_xc_matches_the_oracle(angular):
     run = P.reference_like(45, 9, 20, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=3)
     run = dataclasses.replace(run, xc_frozen=True, angular=angular)
     _fp64_vs_oracle(run, 20)
+
+
+# the int8 form with its angular products on the FP64 tensor cores (ggb_set_angular_fp64): the radial
+# product keeps its int8 slices, so the difference from the oracle is the radial product's alone
+@pytest.mark.parametrize("angular,n_l", [("theta", 32), ("theta", 161), ("reference", 161)])
+def test_int8_with_fp64_angular_tracks_the_oracle(angular, n_l):
+    run = dataclasses.replace(_two_tile_case("Ne3", n_l), angular=angular)
+    ref = propagate(to_oracle(run))
+    tp = TimePropagation([run], precision="split_int8", angular_fp64=True)
+    tp.step(run.n_t)
+    got = tp.observables(0)
+    st, msg = tp.status()
+    tp.close()
+    assert st == 0, msg
+    assert rel_err(got["norm"], ref["norm"]) < TOL_I8
+    assert rel_err(got["dipole"].sum(axis=0), ref["dipole"].sum(axis=0)) < TOL_I8
+
+
+def test_set_angular_fp64_is_refused_by_the_fp64_form():
+    from ggbtddft_b200.engine import GGBError
+    run = P.reference_like(32, 8, 4, "H")
+    tp = TimePropagation([run])
+    with pytest.raises(GGBError):
+        tp._call("ggb_set_angular_fp64", 0, 1)
+    tp.close()
