@@ -347,6 +347,9 @@ def main(argv=None):
                          "one run per grid rung")
     ap.add_argument("--xc-frozen", action="store_true", help="exchange-correlation held at the ground state")
     ap.add_argument("--per-rung", type=int, default=1, help="--argon-ensemble-full: FP64 runs checked per rung")
+    ap.add_argument("--hhe-run", type=int, default=-1,
+                    help="instead: run N of the 256-run H/He scan alone, split form against FP64 (with "
+                         "--sensitivity: FP64 against FP64 from perturbed orbitals too)")
     ap.add_argument("--angular-fp64", action="store_true",
                     help="the split form's angular products on the FP64 tensor cores (ggb_set_angular_fp64)")
     ap.add_argument("--sweep", action="store_true",
@@ -361,6 +364,17 @@ def main(argv=None):
             with open(args.out, "w") as f:
                 f.write(json.dumps(rep) + "\n")
         print(json.dumps({k: v for k, v in rep.items() if k != "per_instance"}))
+        return
+    if args.hhe_run >= 0:
+        run = P.hhe_ensemble(256, seed=0, device="cuda", only=[args.hhe_run])[0]
+        run = dataclasses.replace(run, angular=args.angular)
+        atom = "H" if run.name.startswith("H-") else "He"
+        rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64)
+        rep["config"] = f"H/He scan run {args.hhe_run}: {run.name}, angular {args.angular}"
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(rep) + "\n")
+        print(json.dumps({k: v for k, v in rep.items() if k != "harmonic_rel_err"}))
         return
     if args.hhe_ensemble:
         rep = compare_hhe_ensemble(args.precision, angular=args.angular, angular_fp64=args.angular_fp64)

@@ -41,6 +41,8 @@ struct GroupHost {
   double4* obs_d = nullptr;
   int* step_d = nullptr;
   unsigned* done_d = nullptr;
+  unsigned* fin_cnt_d = nullptr;
+  double* fin_scr_d = nullptr;
   bool needs_init = true;
   GroupArgs args{};
   ThetaArgs theta_args{};        // theta form with n_har > 4 (ggb_theta.cu)
@@ -421,6 +423,7 @@ static int prepare(ggb_ctx* ctx) {
     a.col_run = g.col_run_d; a.col_m = g.col_m_d; a.col_occ = g.col_occ_d; a.runs_of_group = g.runs_d;
     a.runs = ctx->runs_dev;
     a.dens = g.dens_d; a.obs = g.obs_d; a.step = g.step_d; a.status = ctx->status_d; a.done = g.done_d;
+    a.fin_cnt = g.fin_cnt_d; a.fin_scr = g.fin_scr_d;
     a.chain[0] = c0; a.chain[1] = c1;
     a.chain[2] = c2;
     if (ctx->dims.precision != GGB_FP64) {
@@ -567,6 +570,7 @@ int ggb_create(const ggb_dims* dims, const ggb_group_desc* groups, const ggb_run
     if ((rc = dalloc(ctx, &g.r_d, nr)) || (rc = dalloc(ctx, &g.drdx_d, nr)) || (rc = dalloc(ctx, &g.P_d, nr)) ||
         (rc = dalloc(ctx, &g.dens_d, nc * N_DEN * nr)) || (rc = dalloc(ctx, &g.obs_d, 2 * nc * nl * g.n_tiles)) ||
         (rc = dalloc(ctx, &g.step_d, 1)) || (rc = dalloc(ctx, &g.done_d, 1)) ||
+        (rc = dalloc(ctx, &g.fin_cnt_d, g.runs.size())) || (rc = dalloc(ctx, &g.fin_scr_d, nc * FIN_OB * 8)) ||
         (rc = dalloc(ctx, &g.col_run_d, nc)) || (rc = dalloc(ctx, &g.col_m_d, nc)) ||
         (rc = dalloc(ctx, &g.col_occ_d, nc)) || (rc = dalloc(ctx, &g.runs_d, g.runs.size())))
       return bad(rc, "alloc");
@@ -674,6 +678,7 @@ int ggb_set_orbitals(ggb_ctx* ctx, int run, const double* x, const int* l, const
   CK(cudaMemset(r.vexc0_d, 0, nr * sizeof(double)));
   CK(cudaMemset(g.step_d, 0, sizeof(int)));
   CK(cudaMemset(g.done_d, 0, sizeof(unsigned)));
+  CK(cudaMemset(g.fin_cnt_d, 0, g.runs.size() * sizeof(unsigned)));
   r.orb_set = true;
   g.needs_init = true;
   if (ctx->dims.precision != GGB_FP64 && ctx->prepared) {

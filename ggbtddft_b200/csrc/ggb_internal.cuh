@@ -22,6 +22,7 @@ constexpr int TR = 32;            // radii per angular tile (one warp-width, coa
 constexpr int ANG_WARPS = 8;      // warps per angular CTA
 constexpr int MAX_NL = 220;       // largest N_l: two [N_l][32] complex128 tiles fit in 227 KB of shared memory
 constexpr int MAX_NR = 8192;      // largest N_r: three [N_r] FP64 rows of the potentials kernel
+constexpr int FIN_OB = 32;         // observables blocks per run in k_finalize (slices of l)
 constexpr int N_DEN = 4;          // density multipoles carried per column (L = 0..3)
 
 // status bits (sticky, OR-ed on the device)
@@ -103,6 +104,8 @@ struct GroupArgs {
   int* step;                // ctx-wide step counter
   unsigned* status;
   unsigned* done;           // block counter for the last-block step increment
+  unsigned* fin_cnt;        // [n_runs] finished observables blocks of the step (last-block totals)
+  double* fin_scr;          // [n_cols][FIN_OB][8] slice totals of the observables (double-double)
   Chain chain[3];   // first half, second half, empty (initial partials)
 };
 

@@ -526,69 +526,94 @@ __device__ __forceinline__ double ipow(double x, int L) {
 }
 
 // Blocks: for each run of the group, n_den Hartree blocks (L = 0..n_den-1; block L = 0 also does
-// the exchange potential) + 1 observables block.  mode 0 = initial potentials (no observables,
-// no step increment), mode 1 = end of step, mode 2 = end of step without observables or step
-// increment (profiling).
+// the exchange potential) + FIN_OB observables blocks.  mode 0 = initial potentials (no observables,
+// no step increment), mode 1 = end of step, mode 2 = end of step without the step increment and the
+// watchdog checks (the per-phase timing).
+//
+// Observables: observables block ob sums the partials of a slice of l (one warp per orbital, lanes
+// striding over the tiles, double-double), writes the per-l series and its slice's totals to a
+// scratch row; the last of the run's FIN_OB blocks to finish (a per-run counter) adds the slices in
+// order, writes the totals and the norm and runs the NaN / norm-growth watchdog.
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode) {
   extern __shared__ double fsm[];  // [3][N_r]
   __shared__ dd wsum[FIN_THREADS / 32];
-  const int nb = g.n_den + 1;
+  __shared__ int s_last;
+  const int nb = g.n_den + FIN_OB;
   const int ri = blockIdx.x / nb;
-  const int role = blockIdx.x - ri * nb;  // < n_den: Hartree L = role; == n_den: observables
+  const int role = blockIdx.x - ri * nb;  // < n_den: Hartree L = role; >= n_den: observables slice
   const int run_idx = g.runs_of_group[ri];
   RunDev run = g.runs[run_idx];
   const int n_r = g.n_r, n_l = g.n_l, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   const int step = *g.step;
-  const bool obs_block = (role == g.n_den);
+  const bool obs_block = role >= g.n_den;
+  const int ob = role - g.n_den;
 
-  if (obs_block && mode == 1) {
+  if (obs_block && mode != 0) {
     if (step >= run.n_t) {
-      if (tid == 0) atomicOr(g.status, ST_STEP_OVERFLOW);
+      if (mode == 1 && ob == 0 && tid == 0) atomicOr(g.status, ST_STEP_OVERFLOW);
     } else {
       const int n_orb = run.n_orb;
-      // per (l, orbital): compensated sum over r tiles
-      for (int idx = tid; idx < n_l * n_orb; idx += FIN_THREADS) {
-        const int l = idx / n_orb, k = idx - l * n_orb;
-        const double4* p = g.obs + 2 * (((size_t)(run.col0 + k) * n_l + l) * g.n_tiles);
-        dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
-        for (int t = 0; t < g.n_tiles; ++t) {
-          const double4 h = p[2 * t], lo = p[2 * t + 1];
-          sx = dd_add(sx, dd{h.x, lo.x}); sy = dd_add(sy, dd{h.y, lo.y});
-          sz = dd_add(sz, dd{h.z, lo.z}); sw = dd_add(sw, dd{h.w, lo.w});
+      const int l0 = ob * n_l / FIN_OB, l1 = (ob + 1) * n_l / FIN_OB;
+      for (int k = warp; k < n_orb; k += FIN_THREADS / 32) {
+        dd tx{0.0, 0.0}, ty{0.0, 0.0}, tz{0.0, 0.0}, tw{0.0, 0.0};
+        for (int l = l0; l < l1; ++l) {
+          const double4* p = g.obs + 2 * (((size_t)(run.col0 + k) * n_l + l) * g.n_tiles);
+          dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
+          for (int t = lane; t < g.n_tiles; t += 32) {
+            const double4 h = p[2 * t], lo = p[2 * t + 1];
+            sx = dd_add(sx, dd{h.x, lo.x}); sy = dd_add(sy, dd{h.y, lo.y});
+            sz = dd_add(sz, dd{h.z, lo.z}); sw = dd_add(sw, dd{h.w, lo.w});
+          }
+          sx = warp_sum_dd2(sx); sy = warp_sum_dd2(sy); sz = warp_sum_dd2(sz); sw = warp_sum_dd2(sw);
+          if (lane == 0 && g.per_l) {
+            run.dip[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
+            run.acc[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
+          }
+          tx = dd_add(tx, sx); ty = dd_add(ty, sy); tz = dd_add(tz, sz); tw = dd_add(tw, sw);
         }
-        if (g.per_l) {
-          run.dip[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
-          run.acc[((size_t)l * n_orb + k) * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
+        if (lane == 0) {
+          double* o = g.fin_scr + ((size_t)(run.col0 + k) * FIN_OB + ob) * 8;
+          o[0] = tx.hi; o[1] = tx.lo; o[2] = ty.hi; o[3] = ty.lo;
+          o[4] = tz.hi; o[5] = tz.lo; o[6] = tw.hi; o[7] = tw.lo;
         }
       }
-      // per orbital: totals over l and the norm; one warp per orbital
-      const int lane = tid & 31, warp = tid >> 5;
-      for (int k = warp; k < n_orb; k += FIN_THREADS / 32) {
-        const double4* p = g.obs + 2 * ((size_t)(run.col0 + k) * n_l * g.n_tiles);
-        dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
-        for (int q = lane; q < n_l * g.n_tiles; q += 32) {
-          const double4 h = p[2 * q], lo = p[2 * q + 1];
-          sx = dd_add(sx, dd{h.x, lo.x}); sy = dd_add(sy, dd{h.y, lo.y});
-          sz = dd_add(sz, dd{h.z, lo.z}); sw = dd_add(sw, dd{h.w, lo.w});
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(g.fin_cnt + ri, 1u) == (unsigned)(FIN_OB - 1);
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        // totals over l (the slices in order), the norm; one warp per orbital
+        for (int k = warp; k < n_orb; k += FIN_THREADS / 32) {
+          dd sx{0.0, 0.0}, sy{0.0, 0.0}, sz{0.0, 0.0}, sw{0.0, 0.0};
+          for (int b = 0; b < FIN_OB; ++b) {
+            const double* o = g.fin_scr + ((size_t)(run.col0 + k) * FIN_OB + b) * 8;
+            sx = dd_add(sx, dd{__ldcg(o + 0), __ldcg(o + 1)}); sy = dd_add(sy, dd{__ldcg(o + 2), __ldcg(o + 3)});
+            sz = dd_add(sz, dd{__ldcg(o + 4), __ldcg(o + 5)}); sw = dd_add(sw, dd{__ldcg(o + 6), __ldcg(o + 7)});
+          }
+          const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;  // L = 0 row
+          dd nd{0.0, 0.0};
+          for (int q = lane; q < n_r; q += 32) nd = dd_add(nd, dd{dn[q], 0.0});
+          nd = warp_sum_dd2(nd);
+          const double nrm = nd.hi + nd.lo;
+          if (lane == 0) {
+            run.dip_tot[(size_t)k * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
+            run.acc_tot[(size_t)k * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
+            run.norm[(size_t)k * run.n_t + step] = nrm;
+            if (mode == 1) {
+              if (!(nrm == nrm) || isinf(nrm) || !(sx.hi == sx.hi) || !(sz.hi == sz.hi)) atomicOr(g.status, ST_NAN);
+              if (nrm > run.norm0[k] * (1.0 + g.norm_tol) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
+            }
+          }
         }
-        sx = warp_sum_dd2(sx); sy = warp_sum_dd2(sy); sz = warp_sum_dd2(sz); sw = warp_sum_dd2(sw);
-        const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;  // L = 0 row
-        dd nd{0.0, 0.0};
-        for (int q = lane; q < n_r; q += 32) nd = dd_add(nd, dd{dn[q], 0.0});
-        nd = warp_sum_dd2(nd);
-        const double nrm = nd.hi + nd.lo;
-        if (lane == 0) {
-          run.dip_tot[(size_t)k * run.n_t + step] = make_double2(sx.hi + sx.lo, sy.hi + sy.lo);
-          run.acc_tot[(size_t)k * run.n_t + step] = make_double2(sz.hi + sz.lo, sw.hi + sw.lo);
-          run.norm[(size_t)k * run.n_t + step] = nrm;
-          if (!(nrm == nrm) || isinf(nrm) || !(sx.hi == sx.hi) || !(sz.hi == sz.hi)) atomicOr(g.status, ST_NAN);
-          if (nrm > run.norm0[k] * (1.0 + g.norm_tol) + 1e-300) atomicOr(g.status, ST_NORM_GROWTH);
-        }
+        if (tid == 0) g.fin_cnt[ri] = 0u;   // for the next launch (stream-ordered after this one)
       }
     }
-  } else if (obs_block && mode == 0) {
+  } else if (obs_block && mode == 0 && ob == 0) {
     // initial norm for the growth watchdog
-    const int lane = tid & 31, warp = tid >> 5;
     for (int k = warp; k < run.n_orb; k += FIN_THREADS / 32) {
       const double* dn = g.dens + (size_t)(run.col0 + k) * N_DEN * n_r;
       dd nd{0.0, 0.0};
@@ -628,8 +653,8 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
     }
   }
 
-  // exchange (block L = 0, or the observables block when Hartree is off)
-  const bool xc_block = (g.n_den > 0) ? (role == 0) : obs_block;
+  // exchange (block L = 0, or the first observables block when Hartree is off)
+  const bool xc_block = (g.n_den > 0) ? (role == 0) : (ob == 0);
   if (xc_block) {
     const bool pw92 = (run.flags & RUN_FLAG_PW92) != 0;
     for (int q = tid; q < n_r; q += FIN_THREADS) {
@@ -689,7 +714,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(GroupArgs g, int mode)
 }
 
 void launch_finalize(const GroupArgs& g, int mode, cudaStream_t s) {
-  const dim3 grid(g.n_runs * (g.n_den + 1)), block(FIN_THREADS);
+  const dim3 grid(g.n_runs * (g.n_den + FIN_OB)), block(FIN_THREADS);
   const size_t smem = 3 * (size_t)g.n_r * sizeof(double);
   k_finalize<<<grid, block, smem, s>>>(g, mode);
 }
