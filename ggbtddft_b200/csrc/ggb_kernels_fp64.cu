@@ -352,16 +352,30 @@ k_radial_fp64(int n_r, int n_cols, int n_l, const double2* __restrict__ W, const
       }
     }
   } else {
-    // consumers: thread t computes output radius i0 + t for the tile's TC columns
-    const int t = threadIdx.x;
+    // consumers on the FP64 tensor cores: warp w computes output radii i0 + 32 w .. + 31 (four 8-row
+    // MMA tiles) for the tile's TC columns.  Real form of the complex product, columns interleaved
+    // (2 c + 0/1 = real/imaginary part of column c):  [Yr Yi] = Wr B + Wi B'  with B = [Xr Xi] and
+    // B' = [-Xi Xr] per column, so that a thread's two accumulators of an 8-column tile are one
+    // complex output.  A (i, k) = W[l][k][i] from the W rows in shared memory (one 16-byte load
+    // gives the Wr and Wi fragments), B and B' from one 16-byte load of x.  k beyond the row (the
+    // last chunk) contributes zero on both sides.
+    constexpr int NT = (2 * TC + 7) / 8;            // 8-column MMA tiles
+    const int g8 = lane >> 2, q = lane & 3;
     int it = 0;
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
       const int ct = tile % n_ct, rest = tile / n_ct, itile = rest % n_it, l = rest / n_it;
       const int i0 = itile * RAD_TI;
       const int c0 = ct * TC, nc = min(TC, n_cols - c0);
-      double2 acc[TC];
+      // separate accumulators for the Wr and Wi products (up to 24 columns; beyond, the registers
+      // would spill): the 2 x 4 x NT MMAs of a k step are independent, where one accumulator chain
+      // makes every second MMA wait for the first
+      constexpr bool SPLIT = NT <= 3;
+      double acc[4][NT][2], acd[4][NT][2];
+      auto& adst = SPLIT ? acd : acc;
 #pragma unroll
-      for (int c = 0; c < TC; ++c) acc[c] = make_double2(0.0, 0.0);
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = acd[mt][nt][0] = acd[mt][nt][1] = 0.0;
       bool ok = true;
       for (int kc = 0; kc < n_kc; ++kc, ++it) {
         const int s = it % RAD_STAGES;
@@ -372,37 +386,47 @@ k_radial_fp64(int n_r, int n_cols, int n_l, const double2* __restrict__ W, const
         const int kn = min(RAD_KC, n_r - kc * RAD_KC);
         const double2* ws = rsm + (size_t)s * (W_STAGE + X_STAGE);
         const double2* xs = ws + W_STAGE;
-        if (kn == RAD_KC) {
-#pragma unroll 4
-          for (int kk = 0; kk < RAD_KC; ++kk) {
-            const double2 w = ws[kk * RAD_TI + t];
 #pragma unroll
-            for (int c = 0; c < TC; ++c) {
-              const double2 x = xs[c * RAD_KC + kk];
-              acc[c].x = fma(w.x, x.x, fma(-w.y, x.y, acc[c].x));
-              acc[c].y = fma(w.x, x.y, fma(w.y, x.x, acc[c].y));
-            }
-          }
-        } else {
-          for (int kk = 0; kk < kn; ++kk) {
-            const double2 w = ws[kk * RAD_TI + t];
+        for (int ks = 0; ks < RAD_KC / 4; ++ks) {
+          const int kk = 4 * ks + q;
+          const bool kv = kk < kn;
+          double ar[4], ai[4], bp[NT], bq[NT];
 #pragma unroll
-            for (int c = 0; c < TC; ++c) {
-              const double2 x = xs[c * RAD_KC + kk];
-              acc[c].x = fma(w.x, x.x, fma(-w.y, x.y, acc[c].x));
-              acc[c].y = fma(w.x, x.y, fma(w.y, x.x, acc[c].y));
-            }
+          for (int mt = 0; mt < 4; ++mt) {
+            const double2 w = kv ? ws[kk * RAD_TI + 32 * warp + 8 * mt + g8] : make_double2(0.0, 0.0);
+            ar[mt] = w.x;
+            ai[mt] = w.y;
           }
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) {
+            const int c = 4 * nt + (g8 >> 1);
+            const double2 x = (kv && c < TC) ? xs[c * RAD_KC + kk] : make_double2(0.0, 0.0);
+            bp[nt] = (g8 & 1) ? x.y : x.x;
+            bq[nt] = (g8 & 1) ? x.x : -x.y;
+          }
+#pragma unroll
+          for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+              mma_f64_8x8x4(acc[mt][nt][0], acc[mt][nt][1], ar[mt], bp[nt]);
+              mma_f64_8x8x4(adst[mt][nt][0], adst[mt][nt][1], ai[mt], bq[nt]);
+            }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty_bar[s]);
       }
       if (!ok) break;
-      const int i = i0 + t;
-      if (i < n_r)
 #pragma unroll
-        for (int c = 0; c < TC; ++c)
-          if (c < nc) xout[((size_t)l * n_cols + c0 + c) * n_r + i] = acc[c];
+      for (int mt = 0; mt < 4; ++mt) {
+        const int i = i0 + 32 * warp + 8 * mt + g8;
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const int c = 4 * nt + q;
+          if (i < n_r && c < nc)
+            xout[((size_t)l * n_cols + c0 + c) * n_r + i] =
+                make_double2(acc[mt][nt][0] + acd[mt][nt][0], acc[mt][nt][1] + acd[mt][nt][1]);
+        }
+      }
     }
   }
   __syncthreads();
