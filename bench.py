@@ -264,11 +264,11 @@ TRAFFIC_SOURCE = ("per group: algorithmic bytes x (DRAM bytes / algorithmic byte
                   "kernel on ar16-n600 (one M tile, radial) or ar16-n400-l160 (two M tiles)")
 
 
-def measured_traffic(runs, groups, precision, phase):
+def measured_traffic(runs, groups, precision, phase, theta_reuse: bool = False):
     """Estimated DRAM bytes of one launch of `phase` (all groups), or None without a capture."""
     total = 0.0
     for members in groups:
-        sub = phase_traffic(runs, [members], precision)[phase]["bytes"]
+        sub = phase_traffic(runs, [members], precision, theta_reuse)[phase]["bytes"]
         m_tiles = 1 if runs[members[0]].n_l <= 128 else 2
         ratio = MEASURED_TRAFFIC_RATIO.get((precision, phase, m_tiles))
         if ratio is None:
@@ -288,7 +288,7 @@ def chain_products(run) -> int:
     return k + 1
 
 
-def phase_traffic(runs, groups, precision):
+def phase_traffic(runs, groups, precision, theta_reuse: bool = False):
     """Algorithmic bytes and flops of each phase of one step, summed over the grid groups.
 
     radial: W once per group (16 B per complex FP64, 12 B as three BF16 planes per real part, 8 B as
@@ -297,6 +297,9 @@ def phase_traffic(runs, groups, precision):
     column (the split products are not counted).
     angular half: orbitals in and out (cb B each); (#chain GEMMs) x 4 N_l^2 N_r flops per column.
     cb = 16 B for the FP64 and int8 forms (complex128 orbitals), 8 B for the BF16 form.
+    theta_reuse (split_int8, theta form, ggb_set_theta_reuse): the first half runs one product
+    fewer (it starts from the node-basis vectors the second half kept), and the second half also
+    writes those vectors (cb B per value).
     """
     cb = 8 if precision == "split_bf16" else 16
     xin = 12 if precision == "split_int8" else cb
@@ -310,9 +313,12 @@ def phase_traffic(runs, groups, precision):
         n_gemm = chain_products(r0)
         out["radial"]["bytes"] += wb * n_r * n_r * n_l + (xin + cb) * elems
         out["radial"]["flops"] += 8.0 * n_r * n_r * n_l * cols
+        reuse = theta_reuse and precision == "split_int8" and getattr(r0, "angular", "reference") == "theta"
         for k in ("angular_first", "angular_second"):
             out[k]["bytes"] += 2 * cb * elems
-            out[k]["flops"] += n_gemm * 4.0 * n_l * n_l * n_r * cols
+            out[k]["flops"] += (n_gemm - (1 if reuse and k == "angular_first" else 0)) * 4.0 * n_l * n_l * n_r * cols
+        if reuse:
+            out["angular_second"]["bytes"] += cb * elems
     return out
 
 
@@ -361,10 +367,16 @@ def run_ours(args, rank, world, dist):
     units_per_step = sum(r.n_orb for r in runs)
     tp = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t,
                          autotune=bool(args.autotune) and precision == "split_int8",
-                         angular_fp64=args.angular_arith == "fp64")
+                         angular_fp64=args.angular_arith == "fp64", theta_reuse=bool(args.theta_reuse))
+    # basis reuse is active where the int8 angular chain runs the theta form
+    reuse = tp.theta_reuse and not tp.angular_fp64 and args.angular == "theta"
     if precision == "split_int8":
         desc = dict(desc, angular_products="FP64 tensor cores (mma.sync m8n8k4 f64)" if tp.angular_fp64 else
                     "int8 slice products on tcgen05 (31-bit operands, exact int32 accumulation)")
+        if args.angular == "theta" and not tp.angular_fp64:
+            desc = dict(desc, basis_reuse=("on: each first half starts from the node-basis vectors the previous "
+                                           "second half kept (3 angular products per step instead of 4)")
+                        if reuse else "off: 4 angular products per step")
     stream = torch.cuda.Stream()
     h = stream.cuda_stream
     hbm_peak, _, peak_kind = read_peaks()
@@ -409,7 +421,7 @@ def run_ours(args, rank, world, dist):
     if not args.e2e:
         e2e_value, h2d, d2h = None, 0, 0
     tp2 = TimePropagation(runs, precision=precision, per_l=True, n_t=n_t, tuning=tp.tuning,
-                          angular_fp64=tp.angular_fp64) if args.e2e else None
+                          angular_fp64=tp.angular_fp64, theta_reuse=tp.theta_reuse) if args.e2e else None
     if tp2 is not None:
         tp2.step(args.warmup)
         torch.cuda.synchronize()
@@ -433,7 +445,7 @@ def run_ours(args, rank, world, dist):
     # precision's peak).  The peaks of the arithmetic are this GPU's, measured by the library's own
     # microbenchmarks before the timed region; the HBM peak is the measured copy bandwidth.  The int8
     # form's executed slice products (10 per algorithmic real product) are a secondary figure.
-    tf = phase_traffic(runs, tp.groups, precision)
+    tf = phase_traffic(runs, tp.groups, precision, reuse)
     dom = max(("radial", "angular_first", "angular_second"), key=lambda k: phase_ms[k])
     arith_peak = {"fp64": peaks["fp64_tflops"], "split_int8": peaks["int8_tops"],
                   "split_bf16": read_peaks()[1]}[precision]
@@ -465,7 +477,7 @@ def run_ours(args, rank, world, dist):
                                         "k_angular_i8 (tcgen05 kind::i8 chain, FP64 phases)")}}
     d = kernels[dom]
     kname = names["radial" if dom == "radial" else "angular"][precision]
-    est = measured_traffic(runs, tp.groups, precision, dom)
+    est = measured_traffic(runs, tp.groups, precision, dom, reuse)
     roofline = dict(bound="hbm", kernel=f"{dom} ({kname})", achieved=d["gbs"], peak=hbm_peak, unit="GB/s",
                     frac=d["hbm_frac"], traffic=None if est is None else int(est),
                     traffic_source=None if est is None else TRAFFIC_SOURCE,
@@ -616,6 +628,10 @@ def main():
     ap.add_argument("--angular-arith", default=DEFAULT_ANGULAR_ARITH, choices=["int8", "fp64"],
                     help="split_int8 form: the angular products as int8 slice products on tcgen05 (int8) or on "
                          "the FP64 tensor cores with mma.sync (fp64); the radial product stays int8")
+    ap.add_argument("--theta-reuse", type=int, default=1,
+                    help="split_int8 theta form: 1 starts each step's first angular half from the node-basis "
+                         "vectors kept by the previous second half (one product instead of two; "
+                         "ggb_set_theta_reuse), 0 runs both products of every half")
     ap.add_argument("--clocks-csv", default=None,
                     help="where to keep the nvidia-smi clock samples of the timed region (default: a temp dir)")
     ap.add_argument("--e2e", type=int, default=1, help="also measure the end-to-end (host buffers) number")

@@ -760,6 +760,16 @@ int ggb_set_angular_fp64(ggb_ctx* ctx, int group, int on) {
   return GGB_OK;
 }
 
+int ggb_set_theta_reuse(ggb_ctx* ctx, int group, int on) {
+  if (!ctx) return GGB_ERR_ARG;
+  if (group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, GGB_ERR_ARG, "group %d out of range", group);
+  if (ctx->dims.precision != GGB_SPLIT_INT8)
+    return fail(ctx, GGB_ERR_STATE, "ggb_set_theta_reuse applies to the split_int8 form only");
+  if (ctx->prepared) return fail(ctx, GGB_ERR_STATE, "ggb_set_theta_reuse after the first ggb_step");
+  ctx->groups[group].mixed.i8.theta_reuse = on != 0;
+  return GGB_OK;
+}
+
 int ggb_launch_phase(ggb_ctx* ctx, int phase, void* stream) {
   if (!ctx) return GGB_ERR_ARG;
   if (phase < 0 || phase > 3) return fail(ctx, GGB_ERR_ARG, "phase %d outside 0..3", phase);

@@ -429,6 +429,10 @@ struct Ang8Args {
   int ld_stage;           // row length of the FP64 staging tiles [NP][ld_stage] (odd when it fits)
   int n_mats;             // chain matrices per variant
   int n_var;              // dithered variants of the chain matrices (a power of two)
+  // theta form: the node-basis vectors of the second half after its phase, [N_l][n_cols][N_r]
+  // (nullptr: not kept), and the step whose first half may start from them (-1: none)
+  double2* yth;
+  int* yth_step;
 };
 
 // Byte offset of (row n, k) of slice plane 0 in the B operand: per 128-wide k atom, the four slice
@@ -484,6 +488,15 @@ __device__ __forceinline__ void slice_put(uint8_t* xb, int p, int k, double2 v, 
 // exponent serves the whole chain.  The chain matrices S^T stream through a TMA pipeline, one
 // slice plane per stage.  Orbitals in and out are complex128 (xout may alias xin: each CTA reads
 // its whole tile before it writes).
+//
+// Basis reuse (theta form, t.yth set): a half-step is x <- V diag(phase) V^T x with V orthogonal,
+// and nothing acts on the orbitals between the second half of one step and the first half of the
+// next (the potentials only change the phase).  So V^T x at the start of the next first half is
+// the second half's node-basis vector after its phase, which the second half keeps (t.yth, one
+// FP64 copy); the next first half loads it, applies its own phase in the prologue and runs only
+// its last product, one product instead of two.  The skipped pair V^T V is the identity up to the
+// int8 operands' rounding (~2^-31 of each row), which is then not applied.  t.yth_step names the
+// step that may start from the kept vectors; setting orbitals invalidates it.
 template <int NP, bool SECOND_HALF, bool THETA>
 __global__ void __launch_bounds__(A8_THREADS, 2)
 k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, const double2* xin, double2* xout) {
@@ -517,6 +530,11 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   const int step = step_raw < run.n_t ? step_raw : run.n_t - 1;
   const double hdt = 0.5 * g.dt;
   const double* pco = g.coef + ((size_t)CF_P * g.n_m + m) * n_l;
+  // basis reuse: the second half keeps its node-basis vectors, the first half of the step they
+  // were kept for starts from them at its last product (o0 = 1, the theta chain having two)
+  const bool keep_theta = THETA && SECOND_HALF && t.yth != nullptr;
+  const bool from_theta = THETA && !SECOND_HALF && t.yth != nullptr && *t.yth_step == step_raw;
+  const int o0 = from_theta ? 1 : 0;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < t.stages; ++s) {
@@ -559,13 +577,16 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   {
     constexpr int U = 4;
     double part = 0.0;          // this thread's points are fixed: p = threadIdx.x % NP (A8_THREADS % NP == 0)
+    const double2* src = from_theta ? t.yth : xin;
+    // the reuse path applies the first product's phase here, as its epilogue would (same angle)
+    const double* Dv0 = g.dph + ((size_t)ch.ops[0].coupling * g.n_m + m) * g.ldS;
     for (int base = threadIdx.x; base < n_l * NP; base += U * A8_THREADS) {
       double2 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int idx = base + u * A8_THREADS;
         const int l = idx / NP, p = idx - l * NP, r = r0 + p;
-        v[u] = (idx < n_l * NP && r < g.n_r) ? xin[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
+        v[u] = (idx < n_l * NP && r < g.n_r) ? src[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -574,6 +595,12 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
           const int l = idx / NP, p = idx - l * NP;
           double2 w = v[u];
           if (SECOND_HALF && ch.pre_s) w = rotd(w, pbase[4][p] + pco[l] * pbase[2][p]);
+          if (!SECOND_HALF && THETA && from_theta && l >= m) {
+            const double dj = Dv0[l], p2j = legendre_p2(dj), p3j = legendre_p3(dj);
+            double ang = pbase[1][p] * dj + pbase[2][p] * p2j + pbase[3][p] * p3j + pbase[4][p];
+            if (g.theta_tab && r0 + p < g.n_r) ang += run.htab[((size_t)m * n_l + l) * g.n_r + r0 + p] * hdt;
+            w = rotd(w, ang);
+          }
           stg[p * ldf + l] = w;
           part += w.x * w.x + w.y * w.y;
         }
@@ -607,7 +634,7 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     if (lane == 0) {
       int it = 0;
       bool ok = true;
-      for (int o = 0; o < n_ops && ok; ++o) {
+      for (int o = o0; o < n_ops && ok; ++o) {
         const int mat = ch.ops[o].mat + (step_raw & (t.n_var - 1)) * t.n_mats;   // this step's variant
         // stage pa takes slice plane pa; the ring turns once per (tile, atom)
         for (int mt = 0; mt < t.m_tiles && ok; ++mt)
@@ -642,8 +669,8 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
       const uint64_t adesc = sdesc_kmajor(smem_u32(sst), 128, 2);
       const uint64_t bdesc = sdesc_kmajor(smem_u32(xb), 128, 2);
       int round = 0;
-      for (int o = 0; o < n_ops; ++o) {
-        if (o > 0 && !mbar_wait(&xb_bar, (o - 1) & 1, abort_p)) break;
+      for (int o = o0; o < n_ops; ++o) {
+        if (o > o0 && !mbar_wait(&xb_bar, (o - o0 - 1) & 1, abort_p)) break;
         tc_fence_after();
         bool ok = true;
         for (int mt = 0; mt < t.m_tiles && ok; ++mt) {
@@ -686,12 +713,15 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
     // a warp whose 32 channels are all padding (j >= N_l) does no work: its rows of the next
     // operand stay as the fill left them (zero), and the next product's S^T columns there are zero
     const bool live = 128 * mt + 32 * q < n_l;
-    for (int o = 0; o < n_ops; ++o) {
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_bar, o & 1, abort_p));
+    for (int o = o0; o < n_ops; ++o) {
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_bar, (o - o0) & 1, abort_p));
       tc_fence_after();
       if (!ok) break;
       const ChainOp op = ch.ops[o];
       const bool last = (o == n_ops - 1);
+      // basis reuse: the second half keeps the first product's result after its phase (row j of
+      // this column, from radius r0)
+      double2* const ykeep = (keep_theta && o == 0 && j < n_l) ? t.yth + ((size_t)j * g.n_cols + col) * g.n_r + r0 : nullptr;
       if (!live) {
         if (!last) {
           __syncwarp();
@@ -752,6 +782,10 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
             if (dj != 0.0) v[u] = rotd(v[u], pbase[pb][p] * dj);
           }
           if (post_s) v[u] = rotd(v[u], pbase[4][p] + pj * pbase[2][p]);
+          if (ykeep && r0 + p < g.n_r) {
+            const double sc = pinv[p] * 0x1p-24;
+            ykeep[p] = make_double2(v[u].x * sc, v[u].y * sc);
+          }
           if (!last) {
             if (j < lk) {
               const uint32_t o = a8_off(2 * NP, p, j);
@@ -779,6 +813,9 @@ k_angular_i8(const __grid_constant__ CUtensorMap tmS, GroupArgs g, Ang8Args t, c
   if (abort_flag) {
     if (threadIdx.x == 0) atomicOr(g.status, ST_TC_TIMEOUT);
   } else {
+    // the kept vectors serve the first half of the next step (the step counter advances once
+    // per step, after this kernel)
+    if (keep_theta && blockIdx.x == 0 && threadIdx.x == 0) *t.yth_step = step_raw + 1;
     const double2* xs = reinterpret_cast<const double2*>(smem);
     for (int idx = threadIdx.x; idx < n_l * NP; idx += A8_THREADS) {
       const int l = idx / NP, p = idx - l * NP, r = r0 + p;
@@ -1042,6 +1079,13 @@ int int8_prepare(MixedGroup& mg, GroupArgs& a, const double2* W_fp64, int n_mats
     k_build_st_i8<<<n_mm * rows, 256>>>(a.mats, q.St + nst * v, q.sexp, n_mm, a.n_m, n_l, a.ldS, rows, lk, v,
                                         I8_S_VARIANTS);
   I8_CK(cudaGetLastError());
+  // basis reuse of the theta form (one phase op and one closing product per half); the angular
+  // products on the FP64 kernel keep the full chain
+  if (q.theta_reuse && a.theta && !mg.angular_fp64 && a.chain[0].n_ops == 2 && a.chain[1].n_ops == 2) {
+    I8_CK(cudaMalloc(&q.yth, (size_t)n_l * a.n_cols * n_r * sizeof(double2)));
+    I8_CK(cudaMalloc(&q.yth_step, sizeof(int)));
+    I8_CK(cudaMemset(q.yth_step, 0xFF, sizeof(int)));   // -1: nothing kept yet
+  }
   {
     // the variants follow one another along the matrix index: matrix mat of variant v is mat + v n_mats
     cuuint64_t dims[5] = {(cuuint64_t)lk, (cuuint64_t)rows, I8_SLICES, (cuuint64_t)a.n_m,
@@ -1103,6 +1147,8 @@ void int8_angular(MixedGroup& mg, const GroupArgs& a, int half, const double2* x
   t.ld_stage = q.a_ld;
   t.n_mats = q.n_mats;
   t.n_var = I8_S_VARIANTS;
+  t.yth = q.yth;
+  t.yth_step = q.yth_step;
   const dim3 grid(a.n_cols * ((a.n_r + q.np - 1) / q.np));
 #define GGB_A8(NP, SH, TH) k_angular_i8<NP, SH, TH><<<grid, A8_THREADS, q.a_smem, s>>>(q.tmS, a, t, xin, xout)
   if (q.np == 32) {
@@ -1127,6 +1173,8 @@ void int8_release(I8Group& q) {
   cudaFree(q.xexp);
   cudaFree(q.St);
   cudaFree(q.sexp);
+  cudaFree(q.yth);
+  cudaFree(q.yth_step);
   q = I8Group();
 }
 

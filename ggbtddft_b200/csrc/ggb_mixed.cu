@@ -734,7 +734,12 @@ int mixed_prepare(MixedGroup& m, GroupArgs& a, const double2* W_fp64, double2* x
 
 int mixed_load_orbitals(MixedGroup& m, const GroupArgs& a, const double2* x_fp64) {
   if (!m.ready) return GGB_ERR_STATE;
-  if (m.precision == GGB_SPLIT_INT8) return GGB_OK;   // the state is the FP64 buffer itself
+  if (m.precision == GGB_SPLIT_INT8) {
+    // the state is the FP64 buffer itself; node-basis vectors kept for basis reuse no longer match it
+    if (!m.i8.yth_step) return GGB_OK;
+    if (cudaMemset(m.i8.yth_step, 0xFF, sizeof(int)) != cudaSuccess) return GGB_ERR_CUDA;
+    return cudaDeviceSynchronize() == cudaSuccess ? GGB_OK : GGB_ERR_CUDA;
+  }
   const size_t n = (size_t)a.n_l * a.n_cols * a.n_r;
   k_d2f<<<512, 256>>>(x_fp64, m.X, n);
   return cudaDeviceSynchronize() == cudaSuccess ? GGB_OK : GGB_ERR_CUDA;

@@ -33,6 +33,11 @@ struct I8Group {
   size_t smem = 0;
   int np = 32, a_k_atoms = 0, a_m_tiles = 0, a_stages = 0, a_rows = 0, a_ld = 0;
   size_t a_smem = 0;
+  // theta form, basis reuse (ggb_set_theta_reuse, on by default): the second half's node-basis
+  // vectors after its phase [N_l][n_cols][N_r] and the step whose first half starts from them
+  bool theta_reuse = true;
+  double2* yth = nullptr;
+  int* yth_step = nullptr;
 };
 
 struct MixedGroup {

@@ -55,7 +55,7 @@ EXPORTS = ("ggb_create", "ggb_set_grid", "ggb_set_radial_propagators", "ggb_set_
            "ggb_set_field", "ggb_step", "ggb_get_step", "ggb_get_observables", "ggb_get_orbitals",
            "ggb_get_potentials", "ggb_status", "ggb_destroy", "ggb_version", "ggb_launch_phase",
            "ggb_set_tuning", "ggb_observables_noalloc", "ggb_measure_peaks", "ggb_measure_peak_fp64_mma",
-           "ggb_set_angular_fp64")
+           "ggb_set_angular_fp64", "ggb_set_theta_reuse")
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -81,6 +81,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "ggb_launch_phase": ([P, I_, P], I_),
         "ggb_set_tuning": ([P, I_, I_, I_], I_),
         "ggb_set_angular_fp64": ([P, I_, I_], I_),
+        "ggb_set_theta_reuse": ([P, I_, I_], I_),
         "ggb_get_observables": ([P, I_, P, P, P, I_, I_], I_),
         "ggb_get_orbitals": ([P, I_, P], I_),
         "ggb_get_potentials": ([P, I_, P, P, P, P], I_),
@@ -142,11 +143,14 @@ class TimePropagation:
     def __init__(self, runs: Sequence[RunInputs], precision: str = "fp64", per_l: bool = True,
                  n_t: Optional[int] = None, groups: Optional[List[List[int]]] = None, W_device=None,
                  tuning: Optional[Dict[int, Tuple[int, int]]] = None, autotune: bool = False,
-                 angular_fp64: bool = False):
+                 angular_fp64: bool = False, theta_reuse: bool = True):
         """``tuning`` = {group: (radial_bn, radial_stages)} (ggb_set_tuning); ``autotune`` = True
         takes each group's tiles from the autotuner's cache, timing the candidates on a miss
         (split_int8 form only); ``angular_fp64`` = True runs the split_int8 form's angular products
-        on the FP64 tensor cores (ggb_set_angular_fp64), the radial product staying int8."""
+        on the FP64 tensor cores (ggb_set_angular_fp64), the radial product staying int8;
+        ``theta_reuse`` = False runs both products of every angular half in the split_int8 theta
+        form (ggb_set_theta_reuse; by default a step's first half starts from the node-basis
+        vectors its predecessor's second half kept)."""
         self.lib = load_library()
         self.runs = list(runs)
         self.precision = precision
@@ -195,6 +199,10 @@ class TimePropagation:
         if self.angular_fp64:
             for gi in range(len(self.groups)):
                 self._call("ggb_set_angular_fp64", gi, 1)
+        self.theta_reuse = bool(theta_reuse) and precision == "split_int8"
+        if precision == "split_int8" and not self.theta_reuse:
+            for gi in range(len(self.groups)):
+                self._call("ggb_set_theta_reuse", gi, 0)
         for i in range(len(self.runs)):
             self.set_orbitals(i, self.runs[i].x0)
             self.set_field(i, self.runs[i].E)

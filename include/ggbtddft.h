@@ -153,6 +153,17 @@ int ggb_set_tuning(ggb_ctx* ctx, int group, int radial_bn, int radial_stages);
    first step.  No counterpart in the reference. */
 int ggb_set_angular_fp64(ggb_ctx* ctx, int group, int on);
 
+/* split_int8 form, theta form (GGB_RUN_THETA), before the first ggb_step: basis reuse of `group`,
+   on by default.  Each angular half-step is x <- V diag(phase) V^T x with V orthogonal, and nothing
+   acts on the orbitals between one step's second half and the next step's first half, so the first
+   half starts from the second half's node-basis vectors (kept in FP64, one more orbital-sized buffer
+   per group) and runs one product instead of two: three angular products per step instead of four.
+   The omitted pair V^T V is the identity up to the int8 operands' rounding.  Setting orbitals
+   invalidates the kept vectors (that step runs both products).  on = 0 keeps both products of every
+   half.  GGB_ERR_STATE for other forms or after the first step; no effect with ggb_set_angular_fp64
+   or without the theta form.  No counterpart in the reference (its couplings run every product). */
+int ggb_set_theta_reuse(ggb_ctx* ctx, int group, int on);
+
 /* Number of steps taken since the last ggb_set_orbitals (synchronises the context's work). */
 int ggb_get_step(ggb_ctx* ctx, int* step);
 
