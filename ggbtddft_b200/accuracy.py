@@ -35,8 +35,10 @@ from .engine import TimePropagation
 IONISATION_POTENTIAL = {"H": 0.5, "He": 0.9036, "Ar": 0.5792}   # Ha (experimental first Ip)
 
 
-def _run(run: P.RunInputs, precision: str, n_steps: int, chunk: int = 4096, angular_fp64: bool = False):
-    tp = TimePropagation([run], precision=precision, per_l=True, n_t=n_steps, angular_fp64=angular_fp64)
+def _run(run: P.RunInputs, precision: str, n_steps: int, chunk: int = 4096, angular_fp64: bool = False,
+         theta_reuse: bool = True):
+    tp = TimePropagation([run], precision=precision, per_l=True, n_t=n_steps, angular_fp64=angular_fp64,
+                         theta_reuse=theta_reuse)
     t0 = time.perf_counter()
     done = 0
     while done < n_steps:
@@ -77,11 +79,13 @@ def _errors(run, ref, tst, atom, e0):
 
 
 def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_int8", n_steps: Optional[int] = None,
-                  e0: Optional[float] = None, sensitivity: float = 0.0, angular_fp64: bool = False) -> dict:
-    """``angular_fp64``: the split form with its angular products on the FP64 tensor cores."""
+                  e0: Optional[float] = None, sensitivity: float = 0.0, angular_fp64: bool = False,
+                  theta_reuse: bool = True) -> dict:
+    """``angular_fp64``: the split form with its angular products on the FP64 tensor cores;
+    ``theta_reuse`` = False: the split theta form without basis reuse (ggb_set_theta_reuse)."""
     n = run.n_t if n_steps is None else n_steps
     ref = _run(run, "fp64", n)
-    tst = _run(run, precision, n, angular_fp64=angular_fp64)
+    tst = _run(run, precision, n, angular_fp64=angular_fp64, theta_reuse=theta_reuse)
     e0 = float(np.abs(run.E).max()) if e0 is None else e0
     fp64_self = None
     if sensitivity > 0:
@@ -99,7 +103,8 @@ def compare_forms(run: P.RunInputs, atom: str, precision: str = "split_int8", n_
     herr = S.harmonic_errors(s_tst, s_ref, w, run.omega0, q_cut)
     odd = herr[0::2]
     return dict(
-        config=run.name, precision=precision, steps=n, dt=run.dt, omega0=run.omega0, cutoff_order=q_cut,
+        config=run.name, precision=precision, theta_reuse=bool(theta_reuse), steps=n, dt=run.dt,
+        omega0=run.omega0, cutoff_order=q_cut,
         use_hartree=int(run.use_hartree), fp64_self_sensitivity=fp64_self,
         seconds=dict(fp64=ref["seconds"], split=tst["seconds"]),
         status=dict(fp64=ref["status"], split=tst["status"]),
@@ -350,6 +355,11 @@ def main(argv=None):
     ap.add_argument("--hhe-run", type=int, default=-1,
                     help="instead: run N of the 256-run H/He scan alone, split form against FP64 (with "
                          "--sensitivity: FP64 against FP64 from perturbed orbitals too)")
+    ap.add_argument("--argon-run", type=int, default=-1,
+                    help="instead: run N of the 64-run argon focal scan alone over its whole pulse, split form "
+                         "against FP64 (with --frozen, --xc-frozen and --angular as given)")
+    ap.add_argument("--theta-reuse", type=int, default=1,
+                    help="split theta form: 1 with basis reuse (the default), 0 both products of every half")
     ap.add_argument("--angular-fp64", action="store_true",
                     help="the split form's angular products on the FP64 tensor cores (ggb_set_angular_fp64)")
     ap.add_argument("--sweep", action="store_true",
@@ -365,11 +375,25 @@ def main(argv=None):
                 f.write(json.dumps(rep) + "\n")
         print(json.dumps({k: v for k, v in rep.items() if k != "per_instance"}))
         return
+    if args.argon_run >= 0:
+        run = P.argon_ensemble(64, seed=0, device="cuda", only=[args.argon_run], xc_frozen=args.xc_frozen)[0]
+        run = dataclasses.replace(run, angular=args.angular, use_hartree=0 if args.frozen else run.use_hartree)
+        rep = compare_forms(run, "Ar", args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64,
+                            theta_reuse=bool(args.theta_reuse))
+        pot = "all potentials frozen" if args.frozen else ("xc frozen" if args.xc_frozen else "adiabatic")
+        rep["config"] = (f"argon scan run {args.argon_run}: {run.name}, N_r {run.n_r}, l_max {run.n_l - 1}, "
+                         f"angular {args.angular}, {pot}")
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(json.dumps(rep) + "\n")
+        print(json.dumps({k: v for k, v in rep.items() if k != "harmonic_rel_err"}))
+        return
     if args.hhe_run >= 0:
         run = P.hhe_ensemble(256, seed=0, device="cuda", only=[args.hhe_run])[0]
         run = dataclasses.replace(run, angular=args.angular)
         atom = "H" if run.name.startswith("H-") else "He"
-        rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64)
+        rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64,
+                            theta_reuse=bool(args.theta_reuse))
         rep["config"] = f"H/He scan run {args.hhe_run}: {run.name}, angular {args.angular}"
         if args.out:
             with open(args.out, "w") as f:
@@ -405,7 +429,8 @@ def main(argv=None):
         run = dataclasses.replace(run, xc_frozen=True, name=run.name + "-xcfrozen")
     if args.frozen:
         run = dataclasses.replace(run, use_hartree=0, name=run.name + "-frozen")
-    rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64)
+    rep = compare_forms(run, atom, args.precision, sensitivity=args.sensitivity, angular_fp64=args.angular_fp64,
+                        theta_reuse=bool(args.theta_reuse))
     line = json.dumps(rep)
     if args.out:
         with open(args.out, "w") as f:

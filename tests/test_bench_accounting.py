@@ -30,6 +30,26 @@ def test_phase_bytes_and_flops_of_one_int8_group():
     assert tf["angular_second"]["flops"] == 5 * 4.0 * 97 * 97 * 600 * 144
 
 
+def test_basis_reuse_accounting():
+    """split_int8 theta form with basis reuse: the first half runs one product, the second half also
+    writes the kept node-basis vectors; other forms and the reference chain are unchanged."""
+    runs = [_run(600, 96, angular="theta") for _ in range(16)]
+    elems = 600 * 97 * 144
+    off = bench.phase_traffic(runs, [list(range(16))], "split_int8")
+    on = bench.phase_traffic(runs, [list(range(16))], "split_int8", theta_reuse=True)
+    assert off["angular_first"]["flops"] == 2 * 4.0 * 97 * 97 * 600 * 144
+    assert on["angular_first"]["flops"] == 1 * 4.0 * 97 * 97 * 600 * 144
+    assert on["angular_first"]["bytes"] == off["angular_first"]["bytes"] == 2 * 16 * elems
+    assert on["angular_second"]["flops"] == off["angular_second"]["flops"]
+    assert on["angular_second"]["bytes"] == 3 * 16 * elems
+    assert on["radial"] == off["radial"]
+    ref_chain = [_run(600, 96) for _ in range(16)]
+    assert (bench.phase_traffic(ref_chain, [list(range(16))], "split_int8", theta_reuse=True) ==
+            bench.phase_traffic(ref_chain, [list(range(16))], "split_int8"))
+    assert (bench.phase_traffic(runs, [list(range(16))], "fp64", theta_reuse=True) ==
+            bench.phase_traffic(runs, [list(range(16))], "fp64"))
+
+
 def test_traffic_estimate_uses_the_ratio_of_each_groups_kernel():
     runs = [_run(600, 96), _run(600, 96), _run(900, 144)]
     groups = [[0, 1], [2]]
