@@ -355,7 +355,6 @@ static int prepare(ggb_ctx* ctx) {
     n_r_max = std::max(n_r_max, g.d.n_r);
   }
   CK(configure_kernels_fp64(n_l_max, n_r_max));
-  CK(configure_theta(n_l_max));
   for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
     GroupHost& g = ctx->groups[gi];
     if (!g.grid_set) return fail(ctx, GGB_ERR_STATE, "group %zu: grid not set", gi);

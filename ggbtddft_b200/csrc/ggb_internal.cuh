@@ -124,7 +124,6 @@ struct ThetaArgs {
   double* vmp;         // [n_runs][n_mp][N_r]
 };
 void launch_theta_potentials(const GroupArgs& g, const ThetaArgs& t, const double2* x, cudaStream_t s);
-cudaError_t configure_theta(int n_l_max);
 
 __device__ __forceinline__ double2 cmul_conj_phase(double2 x, double eta) {
   // x * exp(-i eta) written as the reference's phase kernels do (couplingP.cuh:99-102)

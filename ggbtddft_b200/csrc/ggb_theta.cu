@@ -27,83 +27,95 @@ namespace ggb {
 
 constexpr int TH_THREADS = 256;
 constexpr int TH_WARPS = TH_THREADS / 32;
-constexpr int TH_QB = 4;          // fine nodes per thread and pass
+constexpr int TH_QB = 2;          // fine nodes per warp
 
-// one block per (run, 32 radii): S and D of the run's orbitals at every positive fine node
+// Work split of the three density/potential kernels: a warp owns 32 radii and a few fine nodes
+// (k_theta_fine), one multipole (k_theta_project) or one node of the phase (k_theta_table), so that
+// a single run (the helium configuration: 13 tiles of 32 radii) still spreads over ~100 blocks; the
+// radii are the lanes, so every load of an orbital, a density or a potential row is coalesced.
+
+// blocks (run, 32 radii, TH_WARPS * TH_QB fine nodes): S and D of the run's orbitals at the block's
+// positive fine nodes, accumulated over the run's orbitals in order in registers
 __global__ void __launch_bounds__(TH_THREADS) k_theta_fine(GroupArgs g, ThetaArgs t, const double2* __restrict__ x) {
-  extern __shared__ double tsm[];           // S [nq][32], D [nq][32]
-  double* S = tsm;
-  double* D = tsm + (size_t)t.nq * 32;
   const int tiles = (g.n_r + 31) / 32;
-  const int ri = blockIdx.x / tiles;
-  const int r0 = (blockIdx.x - ri * tiles) * 32;
+  const int nq = t.nq, n_l = g.n_l;
+  const int qsplit = (nq + TH_WARPS * TH_QB - 1) / (TH_WARPS * TH_QB);
+  const int ri = blockIdx.x / (tiles * qsplit);
+  const int rest = blockIdx.x - ri * tiles * qsplit;
+  const int tile = rest / qsplit, qs = rest - tile * qsplit;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int r = r0 + lane;
-  const bool rv = r < g.n_r;
+  const int r = tile * 32 + lane;
+  const int q0 = (qs * TH_WARPS + warp) * TH_QB;
+  if (r >= g.n_r || q0 >= nq) return;
   const RunDev run = g.runs[g.runs_of_group[ri]];
-  const int n_l = g.n_l, nq = t.nq;
-  for (int i = threadIdx.x; i < 2 * nq * 32; i += TH_THREADS) tsm[i] = 0.0;
-  __syncthreads();
+  double S[TH_QB], D[TH_QB];
+#pragma unroll
+  for (int u = 0; u < TH_QB; ++u) S[u] = D[u] = 0.0;
   for (int k = 0; k < run.n_orb; ++k) {
     const int col = run.col0 + k;
     const int m = g.col_m[col];
     const double occ = (double)g.col_occ[col];
     const double* Tm = t.T + (size_t)m * nq * n_l;
-    for (int q0 = warp * TH_QB; q0 < nq; q0 += TH_WARPS * TH_QB) {
-      double2 e[TH_QB], o[TH_QB];
+    double2 e[TH_QB], o[TH_QB];
 #pragma unroll
-      for (int u = 0; u < TH_QB; ++u) e[u] = o[u] = make_double2(0.0, 0.0);
-      for (int l = m; l < n_l; ++l) {
-        const double2 xv = rv ? x[((size_t)l * g.n_cols + col) * g.n_r + r] : make_double2(0.0, 0.0);
-        const bool odd = ((l - m) & 1) != 0;
-#pragma unroll
-        for (int u = 0; u < TH_QB; ++u) {
-          const int q = q0 + u;
-          const double tv = q < nq ? __ldg(Tm + (size_t)q * n_l + l) : 0.0;
-          if (odd) {
-            o[u].x = fma(tv, xv.x, o[u].x);
-            o[u].y = fma(tv, xv.y, o[u].y);
-          } else {
-            e[u].x = fma(tv, xv.x, e[u].x);
-            e[u].y = fma(tv, xv.y, e[u].y);
-          }
-        }
-      }
+    for (int u = 0; u < TH_QB; ++u) e[u] = o[u] = make_double2(0.0, 0.0);
+    for (int l = m; l < n_l; ++l) {
+      const double2 xv = x[((size_t)l * g.n_cols + col) * g.n_r + r];
+      const bool odd = ((l - m) & 1) != 0;
 #pragma unroll
       for (int u = 0; u < TH_QB; ++u) {
         const int q = q0 + u;
-        if (q < nq) {
-          S[q * 32 + lane] += occ * 2.0 * (e[u].x * e[u].x + e[u].y * e[u].y + o[u].x * o[u].x + o[u].y * o[u].y);
-          D[q * 32 + lane] += occ * 4.0 * (e[u].x * o[u].x + e[u].y * o[u].y);
+        const double tv = q < nq ? __ldg(Tm + (size_t)q * n_l + l) : 0.0;
+        if (odd) {
+          o[u].x = fma(tv, xv.x, o[u].x);
+          o[u].y = fma(tv, xv.y, o[u].y);
+        } else {
+          e[u].x = fma(tv, xv.x, e[u].x);
+          e[u].y = fma(tv, xv.y, e[u].y);
         }
       }
     }
+#pragma unroll
+    for (int u = 0; u < TH_QB; ++u) {
+      S[u] += occ * 2.0 * (e[u].x * e[u].x + e[u].y * e[u].y + o[u].x * o[u].x + o[u].y * o[u].y);
+      D[u] += occ * 4.0 * (e[u].x * o[u].x + e[u].y * o[u].y);
+    }
   }
-  __syncthreads();
-  if (rv) {
-    double* f = t.fine + (size_t)ri * 2 * nq * g.n_r;
-    for (int q = warp; q < nq; q += TH_WARPS) {
-      f[(size_t)q * g.n_r + r] = S[q * 32 + lane];
-      f[((size_t)nq + q) * g.n_r + r] = D[q * 32 + lane];
+  double* f = t.fine + (size_t)ri * 2 * nq * g.n_r;
+#pragma unroll
+  for (int u = 0; u < TH_QB; ++u) {
+    const int q = q0 + u;
+    if (q < nq) {
+      f[(size_t)q * g.n_r + r] = S[u];
+      f[((size_t)nq + q) * g.n_r + r] = D[u];
     }
   }
 }
 
-// one block per (run, 32 radii): rho_L for every L
+// blocks (run, 32 radii, TH_WARPS multipoles): rho_L(r) for the warp's L, four partial sums over
+// the fine nodes
 __global__ void __launch_bounds__(TH_THREADS) k_theta_project(GroupArgs g, ThetaArgs t) {
   const int tiles = (g.n_r + 31) / 32;
-  const int ri = blockIdx.x / tiles;
-  const int r = (blockIdx.x - ri * tiles) * 32 + (threadIdx.x & 31);
-  if (r >= g.n_r) return;
-  const int warp = threadIdx.x >> 5;
-  const double* f = t.fine + (size_t)ri * 2 * t.nq * g.n_r;
-  for (int L = warp; L < t.n_mp; L += TH_WARPS) {
-    const double* src = f + (size_t)(L & 1) * t.nq * g.n_r;
-    const double* w = t.wP + (size_t)L * t.nq;
-    double s = 0.0;
-    for (int q = 0; q < t.nq; ++q) s = fma(__ldg(w + q), src[(size_t)q * g.n_r + r], s);
-    t.rho[((size_t)ri * t.n_mp + L) * g.n_r + r] = s;
+  const int lsplit = (t.n_mp + TH_WARPS - 1) / TH_WARPS;
+  const int ri = blockIdx.x / (tiles * lsplit);
+  const int rest = blockIdx.x - ri * tiles * lsplit;
+  const int tile = rest / lsplit, ls = rest - tile * lsplit;
+  const int r = tile * 32 + (threadIdx.x & 31);
+  const int L = ls * TH_WARPS + (threadIdx.x >> 5);
+  if (r >= g.n_r || L >= t.n_mp) return;
+  const int nq = t.nq, n_r = g.n_r;
+  const double* src = t.fine + ((size_t)ri * 2 + (L & 1)) * nq * n_r + r;
+  const double* w = t.wP + (size_t)L * nq;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int q = 0;
+  for (; q + 3 < nq; q += 4) {
+    s0 = fma(__ldg(w + q), src[(size_t)q * n_r], s0);
+    s1 = fma(__ldg(w + q + 1), src[(size_t)(q + 1) * n_r], s1);
+    s2 = fma(__ldg(w + q + 2), src[(size_t)(q + 2) * n_r], s2);
+    s3 = fma(__ldg(w + q + 3), src[(size_t)(q + 3) * n_r], s3);
   }
+  for (; q < nq; ++q) s0 = fma(__ldg(w + q), src[(size_t)q * n_r], s0);
+  t.rho[((size_t)ri * t.n_mp + L) * n_r + r] = (s0 + s1) + (s2 + s3);
 }
 
 // affine map a -> mul a + add, composed in the order of the recurrence
@@ -172,39 +184,47 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_hartree(GroupArgs g, Theta
   }
 }
 
-// one block per (run, 32 radii): htab[m][j][r] = sum_{L>=1} v_L(r) P_L(x_j^m)
+// blocks (run, 32 radii, TH_WARPS nodes (m, j)): htab[m][j][r] = sum_{L>=1} v_L(r) P_L(x_j^m), four
+// partial sums over L
 __global__ void __launch_bounds__(TH_THREADS) k_theta_table(GroupArgs g, ThetaArgs t) {
   const int tiles = (g.n_r + 31) / 32;
-  const int ri = blockIdx.x / tiles;
-  const int r = (blockIdx.x - ri * tiles) * 32 + (threadIdx.x & 31);
-  if (r >= g.n_r) return;
-  const int warp = threadIdx.x >> 5;
+  const int n_mj = g.n_m * g.n_l;
+  const int jsplit = (n_mj + TH_WARPS - 1) / TH_WARPS;
+  const int ri = blockIdx.x / (tiles * jsplit);
+  const int rest = blockIdx.x - ri * tiles * jsplit;
+  const int tile = rest / jsplit, js = rest - tile * jsplit;
+  const int r = tile * 32 + (threadIdx.x & 31);
+  const int mj = js * TH_WARPS + (threadIdx.x >> 5);
+  if (r >= g.n_r || mj >= n_mj) return;
   const RunDev run = g.runs[g.runs_of_group[ri]];
-  const double* v = t.vmp + (size_t)ri * t.n_mp * g.n_r;
-  for (int mj = warp; mj < g.n_m * g.n_l; mj += TH_WARPS) {
-    const int m = mj / g.n_l, j = mj - m * g.n_l;
-    double s = 0.0;
-    if (j >= m) {
-      const double* pl = t.PLj + (size_t)m * t.n_mp * g.ldS + j;
-      for (int L = 1; L < t.n_mp; ++L) s = fma(v[(size_t)L * g.n_r + r], __ldg(pl + (size_t)L * g.ldS), s);
+  const int n_r = g.n_r, n_mp = t.n_mp;
+  const double* v = t.vmp + (size_t)ri * n_mp * n_r + r;
+  const int m = mj / g.n_l, j = mj - m * g.n_l;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  if (j >= m) {
+    const double* pl = t.PLj + (size_t)m * n_mp * g.ldS + j;
+    int L = 1;
+    for (; L + 3 < n_mp; L += 4) {
+      s0 = fma(v[(size_t)L * n_r], __ldg(pl + (size_t)L * g.ldS), s0);
+      s1 = fma(v[(size_t)(L + 1) * n_r], __ldg(pl + (size_t)(L + 1) * g.ldS), s1);
+      s2 = fma(v[(size_t)(L + 2) * n_r], __ldg(pl + (size_t)(L + 2) * g.ldS), s2);
+      s3 = fma(v[(size_t)(L + 3) * n_r], __ldg(pl + (size_t)(L + 3) * g.ldS), s3);
     }
-    run.htab[(size_t)mj * g.n_r + r] = s;
+    for (; L < n_mp; ++L) s0 = fma(v[(size_t)L * n_r], __ldg(pl + (size_t)L * g.ldS), s0);
   }
+  run.htab[(size_t)mj * n_r + r] = (s0 + s1) + (s2 + s3);
 }
 
 void launch_theta_potentials(const GroupArgs& g, const ThetaArgs& t, const double2* x, cudaStream_t s) {
   const int tiles = (g.n_r + 31) / 32;
-  const size_t smem = 2 * (size_t)t.nq * 32 * sizeof(double);
-  k_theta_fine<<<g.n_runs * tiles, TH_THREADS, smem, s>>>(g, t, x);
-  k_theta_project<<<g.n_runs * tiles, TH_THREADS, 0, s>>>(g, t);
+  const int qsplit = (t.nq + TH_WARPS * TH_QB - 1) / (TH_WARPS * TH_QB);
+  const int lsplit = (t.n_mp + TH_WARPS - 1) / TH_WARPS;
+  const int jsplit = (g.n_m * g.n_l + TH_WARPS - 1) / TH_WARPS;
+  k_theta_fine<<<g.n_runs * tiles * qsplit, TH_THREADS, 0, s>>>(g, t, x);
+  k_theta_project<<<g.n_runs * tiles * lsplit, TH_THREADS, 0, s>>>(g, t);
   const int per_run = (t.n_mp - 1 + TH_WARPS - 1) / TH_WARPS;
   if (per_run > 0) k_theta_hartree<<<g.n_runs * per_run, TH_THREADS, 0, s>>>(g, t);
-  k_theta_table<<<g.n_runs * tiles, TH_THREADS, 0, s>>>(g, t);
-}
-
-cudaError_t configure_theta(int n_l_max) {
-  const size_t smem = 2 * (size_t)n_l_max * 32 * sizeof(double);
-  return cudaFuncSetAttribute((const void*)k_theta_fine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_theta_table<<<g.n_runs * tiles * jsplit, TH_THREADS, 0, s>>>(g, t);
 }
 
 }  // namespace ggb
