@@ -28,6 +28,12 @@ namespace ggb {
 constexpr int TH_THREADS = 256;
 constexpr int TH_WARPS = TH_THREADS / 32;
 constexpr int TH_QB = 2;          // fine nodes per warp
+constexpr int TH_ILP = 8;         // independent partial sums of the projection and table loops
+
+// pairwise sum of the partial sums
+__device__ __forceinline__ double sum_partials(const double (&a)[TH_ILP]) {
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
 
 // Work split of the three density/potential kernels: a warp owns 32 radii and a few fine nodes
 // (k_theta_fine), one multipole (k_theta_project) or one node of the phase (k_theta_table), so that
@@ -92,7 +98,7 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_fine(GroupArgs g, ThetaArg
   }
 }
 
-// blocks (run, 32 radii, TH_WARPS multipoles): rho_L(r) for the warp's L, four partial sums over
+// blocks (run, 32 radii, TH_WARPS multipoles): rho_L(r) for the warp's L, TH_ILP partial sums over
 // the fine nodes
 __global__ void __launch_bounds__(TH_THREADS) k_theta_project(GroupArgs g, ThetaArgs t) {
   const int tiles = (g.n_r + 31) / 32;
@@ -106,16 +112,15 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_project(GroupArgs g, Theta
   const int nq = t.nq, n_r = g.n_r;
   const double* src = t.fine + ((size_t)ri * 2 + (L & 1)) * nq * n_r + r;
   const double* w = t.wP + (size_t)L * nq;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  double acc[TH_ILP];
+#pragma unroll
+  for (int u = 0; u < TH_ILP; ++u) acc[u] = 0.0;
   int q = 0;
-  for (; q + 3 < nq; q += 4) {
-    s0 = fma(__ldg(w + q), src[(size_t)q * n_r], s0);
-    s1 = fma(__ldg(w + q + 1), src[(size_t)(q + 1) * n_r], s1);
-    s2 = fma(__ldg(w + q + 2), src[(size_t)(q + 2) * n_r], s2);
-    s3 = fma(__ldg(w + q + 3), src[(size_t)(q + 3) * n_r], s3);
-  }
-  for (; q < nq; ++q) s0 = fma(__ldg(w + q), src[(size_t)q * n_r], s0);
-  t.rho[((size_t)ri * t.n_mp + L) * n_r + r] = (s0 + s1) + (s2 + s3);
+  for (; q + TH_ILP - 1 < nq; q += TH_ILP)
+#pragma unroll
+    for (int u = 0; u < TH_ILP; ++u) acc[u] = fma(__ldg(w + q + u), src[(size_t)(q + u) * n_r], acc[u]);
+  for (; q < nq; ++q) acc[0] = fma(__ldg(w + q), src[(size_t)q * n_r], acc[0]);
+  t.rho[((size_t)ri * t.n_mp + L) * n_r + r] = sum_partials(acc);
 }
 
 // affine map a -> mul a + add, composed in the order of the recurrence
@@ -184,8 +189,8 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_hartree(GroupArgs g, Theta
   }
 }
 
-// blocks (run, 32 radii, TH_WARPS nodes (m, j)): htab[m][j][r] = sum_{L>=1} v_L(r) P_L(x_j^m), four
-// partial sums over L
+// blocks (run, 32 radii, TH_WARPS nodes (m, j)): htab[m][j][r] = sum_{L>=1} v_L(r) P_L(x_j^m),
+// TH_ILP partial sums over L
 __global__ void __launch_bounds__(TH_THREADS) k_theta_table(GroupArgs g, ThetaArgs t) {
   const int tiles = (g.n_r + 31) / 32;
   const int n_mj = g.n_m * g.n_l;
@@ -200,19 +205,20 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_table(GroupArgs g, ThetaAr
   const int n_r = g.n_r, n_mp = t.n_mp;
   const double* v = t.vmp + (size_t)ri * n_mp * n_r + r;
   const int m = mj / g.n_l, j = mj - m * g.n_l;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  // TH_ILP independent partial sums: the loop is bound by the latency of its loads
+  double acc[TH_ILP];
+#pragma unroll
+  for (int u = 0; u < TH_ILP; ++u) acc[u] = 0.0;
   if (j >= m) {
     const double* pl = t.PLj + (size_t)m * n_mp * g.ldS + j;
     int L = 1;
-    for (; L + 3 < n_mp; L += 4) {
-      s0 = fma(v[(size_t)L * n_r], __ldg(pl + (size_t)L * g.ldS), s0);
-      s1 = fma(v[(size_t)(L + 1) * n_r], __ldg(pl + (size_t)(L + 1) * g.ldS), s1);
-      s2 = fma(v[(size_t)(L + 2) * n_r], __ldg(pl + (size_t)(L + 2) * g.ldS), s2);
-      s3 = fma(v[(size_t)(L + 3) * n_r], __ldg(pl + (size_t)(L + 3) * g.ldS), s3);
-    }
-    for (; L < n_mp; ++L) s0 = fma(v[(size_t)L * n_r], __ldg(pl + (size_t)L * g.ldS), s0);
+    for (; L + TH_ILP - 1 < n_mp; L += TH_ILP)
+#pragma unroll
+      for (int u = 0; u < TH_ILP; ++u)
+        acc[u] = fma(v[(size_t)(L + u) * n_r], __ldg(pl + (size_t)(L + u) * g.ldS), acc[u]);
+    for (; L < n_mp; ++L) acc[0] = fma(v[(size_t)L * n_r], __ldg(pl + (size_t)L * g.ldS), acc[0]);
   }
-  run.htab[(size_t)mj * n_r + r] = (s0 + s1) + (s2 + s3);
+  run.htab[(size_t)mj * n_r + r] = sum_partials(acc);
 }
 
 void launch_theta_potentials(const GroupArgs& g, const ThetaArgs& t, const double2* x, cudaStream_t s) {
