@@ -10,7 +10,8 @@ vectors the second half kept and runs one product instead of two.  The tests che
   with every multipole from the exact quadrature (n_har > 4);
 * after new orbitals are set the steps equal a fresh context's (the kept vectors are invalidated and
   the step counter restarts);
-* batching runs in one grid group still changes nothing at all;
+* batching runs in one grid group, or on several grid groups stepped on concurrent streams, still
+  changes nothing at all;
 * the switch is refused by the FP64 form.
 """
 import dataclasses
@@ -86,6 +87,25 @@ def test_reuse_in_a_group_equals_single_runs():
         assert np.array_equal(ens.observables(i)["dipole"], one.observables(0)["dipole"])
         one.close()
     ens.close()
+
+
+def test_reuse_with_grid_groups_on_concurrent_streams_equals_single_runs():
+    """Runs on different grids form separate groups stepped on their own streams, each with its own
+    kept vectors and step counter: every run equals the run stepped alone."""
+    runs = [_case(32, seed=2),
+            dataclasses.replace(P.reference_like(48, 161, 48, "Ne3", r_mask=15.0, dt_as=10.0, perturb=0.05, seed=5),
+                                angular="theta")]
+    ens = TimePropagation(runs, precision="split_int8")
+    assert len(ens.groups) == 2
+    ens.step(20)
+    for i, r in enumerate(runs):
+        one = TimePropagation([r], precision="split_int8")
+        one.step(20)
+        assert np.array_equal(ens.orbitals(i), one.orbitals(0))
+        one.close()
+    st, msg = ens.status()
+    ens.close()
+    assert st == 0, msg
 
 
 def test_theta_reuse_is_refused_by_the_fp64_form():
