@@ -323,23 +323,27 @@ static int prepare_theta_tables(ggb_ctx* ctx, GroupHost& g, int n_mp) {
         }
       }
     }
-  std::vector<double> lq(n_r, 0.0);
-  for (int a = 1; a < n_r; ++a) lq[a] = (double)std::log((long double)g.r[a - 1] / (long double)g.r[a]);
+  // ratio powers of the Hartree recurrences, fixed by the grid: (r_(a-1)/r_a)^L for L = 0 .. n_mp
+  std::vector<double> rq((size_t)(n_mp + 1) * n_r, 0.0);
+  for (int a = 1; a < n_r; ++a) {
+    const long double lq = std::log((long double)g.r[a - 1] / (long double)g.r[a]);
+    for (int L = 0; L <= n_mp; ++L) rq[(size_t)L * n_r + a] = (double)std::exp((long double)L * lq);
+  }
   ThetaArgs& t = g.theta_args;
   t.n_mp = n_mp;
   t.nq = nq;
-  double *Td, *wPd, *PLd, *lqd, *fine, *rho, *vmp;
+  double *Td, *wPd, *PLd, *rqd, *fine, *rho, *vmp;
   int rc;
   const size_t nrun = g.runs.size();
   if ((rc = dalloc(ctx, &Td, T.size())) || (rc = dalloc(ctx, &wPd, wP.size())) || (rc = dalloc(ctx, &PLd, PLj.size())) ||
-      (rc = dalloc(ctx, &lqd, lq.size())) || (rc = dalloc(ctx, &fine, nrun * 2 * nq * n_r)) ||
+      (rc = dalloc(ctx, &rqd, rq.size())) || (rc = dalloc(ctx, &fine, nrun * 2 * nq * n_r)) ||
       (rc = dalloc(ctx, &rho, nrun * n_mp * n_r)) || (rc = dalloc(ctx, &vmp, nrun * n_mp * n_r)))
     return rc;
   CK(cudaMemcpy(Td, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(wPd, wP.data(), wP.size() * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(PLd, PLj.data(), PLj.size() * sizeof(double), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(lqd, lq.data(), lq.size() * sizeof(double), cudaMemcpyHostToDevice));
-  t.T = Td; t.wP = wPd; t.PLj = PLd; t.lq = lqd; t.fine = fine; t.rho = rho; t.vmp = vmp;
+  CK(cudaMemcpy(rqd, rq.data(), rq.size() * sizeof(double), cudaMemcpyHostToDevice));
+  t.T = Td; t.wP = wPd; t.PLj = PLd; t.rq = rqd; t.fine = fine; t.rho = rho; t.vmp = vmp;
   for (int ri : g.runs) {
     RunHost& r = ctx->runs[ri];
     if ((rc = dalloc(ctx, &r.htab_d, (size_t)n_m * n_l * n_r))) return rc;

@@ -118,7 +118,7 @@ struct ThetaArgs {
   const double* T;     // [N_m][nq][N_l]  Theta_l^m(x_q)
   const double* wP;    // [n_mp][nq]      w_q P_L(x_q)
   const double* PLj;   // [N_m][n_mp][ldS] P_L(x_j^m) at the P coupling's nodes
-  const double* lq;    // [N_r]           log(r_(a-1) / r_a) for a >= 1, 0 at a = 0
+  const double* rq;    // [n_mp+1][N_r]   (r_(a-1) / r_a)^L for a >= 1, 0 at a = 0
   double* fine;        // [n_runs][2][nq][N_r]  S_q = sum occ 2(|E|^2 + |O|^2), D_q = sum occ 4 Re(E conj O)
   double* rho;         // [n_runs][n_mp][N_r]
   double* vmp;         // [n_runs][n_mp][N_r]

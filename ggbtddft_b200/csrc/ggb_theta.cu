@@ -143,10 +143,12 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_hartree(GroupArgs g, Theta
   double* v = t.vmp + ((size_t)ri * t.n_mp + L) * n;
   const int C = (n + 31) / 32;
   const int a0 = lane * C, a1 = min(n, a0 + C);
-  // forward: A_a = f_a A_(a-1) + rho_a, f_a = (r_(a-1)/r_a)^L = exp(L lq_a), f_0 = 0
+  // forward: A_a = f_a A_(a-1) + rho_a, f_a = (r_(a-1)/r_a)^L (the grid's table), f_0 = 0
+  const double* fL = t.rq + (size_t)L * n;
+  const double* gL = t.rq + (size_t)(L + 1) * n;
   Aff mine{1.0, 0.0};
   for (int a = a0; a < a1; ++a) {
-    const double f = a == 0 ? 0.0 : exp((double)L * t.lq[a]);
+    const double f = a == 0 ? 0.0 : fL[a];
     mine = Aff{f * mine.mul, fma(f, mine.add, rho[a])};
   }
   Aff inc = mine;                       // inclusive scan of the lanes' maps, in lane order
@@ -158,17 +160,17 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_hartree(GroupArgs g, Theta
   double A = __shfl_up_sync(0xffffffffu, inc.add, 1);   // A_(a0 - 1): the previous lanes' maps applied to 0
   if (lane == 0) A = 0.0;
   for (int a = a0; a < a1; ++a) {
-    const double f = a == 0 ? 0.0 : exp((double)L * t.lq[a]);
+    const double f = a == 0 ? 0.0 : fL[a];
     A = fma(f, A, rho[a]);
     v[a] = A;
   }
-  // backward: B_a = g_a (B_(a+1) + rho_(a+1)), g_a = (r_a/r_(a+1))^(L+1) = exp((L+1) lq_(a+1)), B_(n-1) = 0;
+  // backward: B_a = g_a (B_(a+1) + rho_(a+1)), g_a = (r_a/r_(a+1))^(L+1), B_(n-1) = 0;
   // lane order reversed: the last chunk first
   const int bl = 31 - lane;
   const int b0 = bl * C, b1 = min(n, b0 + C);
   Aff mb{1.0, 0.0};
   for (int a = b1 - 1; a >= b0; --a) {
-    const double gg = a == n - 1 ? 0.0 : exp((double)(L + 1) * t.lq[a + 1]);
+    const double gg = a == n - 1 ? 0.0 : gL[a + 1];
     const double rn = a == n - 1 ? 0.0 : rho[a + 1];
     mb = Aff{gg * mb.mul, gg * (mb.add + rn)};
   }
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(TH_THREADS) k_theta_hartree(GroupArgs g, Theta
   if (lane == 0) B = 0.0;
   __syncwarp();
   for (int a = b1 - 1; a >= b0; --a) {
-    const double gg = a == n - 1 ? 0.0 : exp((double)(L + 1) * t.lq[a + 1]);
+    const double gg = a == n - 1 ? 0.0 : gL[a + 1];
     const double rn = a == n - 1 ? 0.0 : rho[a + 1];
     B = gg * (B + rn);
     v[a] = (v[a] + B) / g.r[a];
