@@ -45,6 +45,9 @@ CASES = {
                 intensity=2e14, omega0=0.057, cycles=1.0),
     "ne3_64": dict(n_r=64, n_l=32, n_t=64, atom="Ne3", r_mask=20.0, zeta_ref=1.0, dt_as=10.0,
                    intensity=3e14, omega0=0.057, cycles=1.0, perturb=0.05, seed=7),
+    # twice the radial and angular sizes, every coupling and the Hartree/exchange phases active
+    "ne3_128": dict(n_r=128, n_l=64, n_t=48, atom="Ne3", r_mask=30.0, zeta_ref=1.0, dt_as=10.0,
+                    intensity=3e14, omega0=0.057, cycles=1.0, perturb=0.05, seed=11),
 }
 
 
