@@ -48,6 +48,9 @@ CASES = {
     # twice the radial and angular sizes, every coupling and the Hartree/exchange phases active
     "ne3_128": dict(n_r=128, n_l=64, n_t=48, atom="Ne3", r_mask=30.0, zeta_ref=1.0, dt_as=10.0,
                     intensity=3e14, omega0=0.057, cycles=1.0, perturb=0.05, seed=11),
+    # all-electron argon (nine orbitals, m = 0 and 1), every coupling active
+    "ar9_256": dict(n_r=256, n_l=64, n_t=32, atom="Ar9", r_mask=60.0, zeta_ref=2.0 * 0.5 / 90.0,
+                    dt_as=0.02 / 0.041341373335182, intensity=1.4e14, omega0=0.057, cycles=1.0),
 }
 
 

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10   # FP64 form vs the reference / the oracle (relative to the series maximum)
 
 
-@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128"])
+@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128", "ar9_256"])
 def test_fp64_matches_reference_binary(case):
     run, dref = load_ref_case(case)
     out = h_time_propagation(run)

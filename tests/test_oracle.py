@@ -16,7 +16,7 @@ def test_lobatto_nodes_match_shipped_roots(n):
     assert np.max(np.abs(I.lobatto_interior_nodes(n) - ref)) < 5e-15
 
 
-@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128"])
+@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128", "ar9_256"])
 def test_oracle_matches_reference_binary(case):
     """Dipole series of the reference main.cu (sm_100a build, same inputs) vs the oracle."""
     run, dref = load_ref_case(case)
