@@ -6,8 +6,8 @@ A "step" is one time step of every run of the workload (both angular half-steps,
 propagator, density, Hartree/exchange potentials and the dipole/acceleration/norm reductions).
 ``value`` = sum over runs of (orbitals x steps) / device time of the K timed steps, all inputs
 resident in HBM, steps replayed from a captured CUDA graph.  ``e2e`` is the same metric through
-the C ABI from host buffers: orbitals and field uploaded, K steps, per-l dipole/acceleration and
-norm series downloaded, wall clock.
+the C ABI from host buffers: orbitals and field uploaded from pinned host memory, K steps, per-l
+dipole/acceleration and norm series downloaded, wall clock.
 
 Multi-GPU (torchrun): every rank runs an independent replica of the workload (the runs of an
 ensemble are independent; there is no exchange step), ``value`` = all ranks' orbital-steps / the
