@@ -26,6 +26,16 @@ def test_oracle_matches_reference_binary(case):
     assert rel_err(out["dipole"].sum(axis=0), dref.sum(axis=0)) < 1e-10
 
 
+def test_every_reference_case_has_its_fixture_and_its_pin():
+    """Every case oracle/build_ref.py builds from the reference's sources has a committed fixture made
+    from that binary's outputs, and the oracle test above covers it."""
+    from oracle.build_ref import CASES
+    pinned = test_oracle_matches_reference_binary.pytestmark[0].args[1]
+    for name in CASES:
+        assert os.path.exists(os.path.join(GOLDEN, f"ref_{name}.npz")), name
+        assert name in pinned, name
+
+
 def test_p_eigenvalues_are_gauss_legendre_nodes():
     V, D = I.angular_eigensystems(12, 1)["P"]
     nodes, _ = np.polynomial.legendre.leggauss(12)
