@@ -1,6 +1,9 @@
 """The reference's file contract (CPU): workingData inputs, params.cuh and the dipole output files
 written and read back in the reference's layout (ggbtddft_b200/workingdata.py)."""
+import os
+
 import numpy as np
+import pytest
 
 from ggbtddft_b200 import inputs as I
 from ggbtddft_b200 import problems as P
@@ -54,3 +57,25 @@ def test_dipole_outputs_round_trip(tmp_path):
     np.testing.assert_array_equal(WD.read_dipole_outputs(root, 20000101, 3, 0, 2, 5), d)
     np.testing.assert_array_equal(
         np.fromfile(tmp_path / "20000101/00003/timeDependent/field/E000.bin", dtype=np.float64), E)
+
+
+REF_BUILD = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128"])
+def test_reference_run_directory_reproduces_the_reference_binary(case):
+    """The drop-in file contract end to end: the workingData tree and params.cuh that the reference
+    binary of the case read (written by oracle/build_ref.py), loaded with read_working_data (the field
+    generated from the params.cuh values, as h_initialiseField does) and propagated by the oracle, give
+    the dipole files that binary wrote (the committed fixture)."""
+    d = os.path.join(REF_BUILD, case)
+    if not os.path.isdir(os.path.join(d, "run", "workingData")):
+        pytest.skip("reference build of this case not present (oracle/build_ref.py needs the reference sources)")
+    from oracle.step_oracle import propagate
+    from tests.helpers import GOLDEN, rel_err, to_oracle
+    params = WD.parse_params_cuh(os.path.join(d, "params.cuh"))
+    ref = np.load(os.path.join(GOLDEN, f"ref_{case}.npz"))
+    run = WD.read_working_data(os.path.join(d, "run"), params)      # the field from params.cuh
+    out = propagate(to_oracle(run))
+    assert out["dipole"].shape == ref["dipole"].shape
+    assert rel_err(out["dipole"], ref["dipole"]) < 1e-10
