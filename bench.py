@@ -254,11 +254,14 @@ class ClockSampler:
 # committed profiling workloads: ar16-n600 (N_l = 97, the one-M-tile kernel, and the radial product)
 # and ar16-n400-l160 (N_l = 161, the two-M-tile kernel).  The ensemble is too large to capture whole;
 # its traffic is estimated group by group from these ratios (orbital traffic grows in proportion to
-# N_r N_l columns; W in proportion to N_r^2 N_l).
+# N_r N_l columns; W in proportion to N_r^2 N_l).  The two-M-tile angular ratios come from the capture
+# with basis reuse (first half: kept vectors in, orbitals out; second half: orbitals in and out, kept
+# vectors out); the one-M-tile ones from a capture of the two-product form of both halves.
 MEASURED_TRAFFIC_RATIO = {
     ("split_int8", "radial", 1): 554.63 / 514.02, ("split_int8", "radial", 2): 554.63 / 514.02,
     ("split_int8", "angular_first", 1): 212.18 / 268.19, ("split_int8", "angular_second", 1): 241.05 / 268.19,
-    ("split_int8", "angular_first", 2): 243.06 / 296.76, ("split_int8", "angular_second", 2): 291.07 / 296.76,
+    ("split_int8", "angular_first", 2): (149.01 + 104.49) / 296.76,
+    ("split_int8", "angular_second", 2): (150.63 + 279.10) / 445.15,
 }
 TRAFFIC_SOURCE = ("per group: algorithmic bytes x (DRAM bytes / algorithmic bytes) of an ncu capture of the same "
                   "kernel on ar16-n600 (one M tile, radial) or ar16-n400-l160 (two M tiles)")
