@@ -26,7 +26,7 @@ def internal():
     return np.load(os.path.join(GOLDEN, "internal_inputs.npz"))
 
 
-@pytest.mark.parametrize("case", ["h64", "ne3_64"])
+@pytest.mark.parametrize("case", ["h64", "ne3_64", "ne3_128", "ar9_256"])
 def test_field_matches_the_reference_binary(case):
     z = np.load(os.path.join(GOLDEN, f"ref_{case}.npz"))
     c = json.loads(str(z["case"]))
@@ -35,7 +35,8 @@ def test_field_matches_the_reference_binary(case):
     t = I.time_grid(c["n_t"], dt)
     E = I.field_super_gaussian(t, fp["e0"], fp["omega0"], fp["tau0"], fp["cep0"])
     assert E.shape == z["E"].shape
-    assert _rel(E, z["E"]) < 1e-14
+    # relative to the amplitude E0: a short window near t = 0 with CEP pi/2 samples only E ~ E0 w t
+    assert np.abs(E - z["E"]).max() <= 1e-14 * fp["e0"]
 
 
 def test_grid_matches_internal_py(internal):
